@@ -1,0 +1,82 @@
+#!/usr/bin/env bash
+# Build the oracle: the reference KPP generator and, for each mechanism, the
+# reference's own KPP-generated C model with the reference Rosenbrock
+# integrator, plus the CPU restatement (oracle/ros_oracle.c).
+#
+# ORACLE INFRASTRUCTURE ONLY.  Outputs go to oracle/_ref/ (git-ignored; the
+# built files travel with the repository snapshot to the GPU machine, where
+# the reference sources are absent and only these prebuilt libraries are used).
+#
+#   oracle/_ref/kpp                               reference generator
+#   oracle/_ref/<mech>/<mech>_*.c|h               reference-generated model
+#   oracle/_ref/<mech>/libkppref_<mech>.so        -O (reference flags, util/Makefile_c:3)
+#   oracle/_ref/<mech>/libkppref_<mech>_O3.so     -O3 -march=native (timing only)
+#
+# The generator is compiled from the unchanged sources in $KPP_REF/src; only
+# the flex/bison front end is replaced by oracle/refkpp/frontend.c because
+# flex, bison and libfl are not installed.  Usage:
+#   oracle/build_ref.sh [KPP_REF=/path/to/reference] [mech ...]
+set -euo pipefail
+
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+KPP_REF="${KPP_REF:-/root/reference}"
+OUT="$HERE/_ref"
+MECHS=("$@")
+if [ ${#MECHS[@]} -eq 0 ]; then MECHS=(small_strato saprc99); fi
+
+if [ ! -d "$KPP_REF/src" ]; then
+  echo "build_ref: reference sources not found at $KPP_REF; keeping prebuilt $OUT" >&2
+  exit 0
+fi
+
+CC="${CC:-gcc}"
+mkdir -p "$OUT/obj"
+
+# ---- 1. the generator -------------------------------------------------------
+GEN_SRCS=(code code_c code_f77 code_f90 code_matlab debug gen kpp scanner scanutil)
+for f in "${GEN_SRCS[@]}"; do
+  "$CC" -O -w -I"$HERE/refkpp" -I"$KPP_REF/src" -c "$KPP_REF/src/$f.c" -o "$OUT/obj/$f.o"
+done
+"$CC" -O -Wall -Wno-unused-function -I"$HERE/refkpp" -I"$KPP_REF/src" \
+  -c "$HERE/refkpp/frontend.c" -o "$OUT/obj/frontend.o"
+"$CC" "$OUT"/obj/*.o -lm -o "$OUT/kpp"
+
+# ---- 2. per-mechanism reference model ---------------------------------------
+for mech in "${MECHS[@]}"; do
+  d="$OUT/$mech"
+  rm -rf "$d"
+  mkdir -p "$d"
+  # The wrapper selects the C language, the reference Rosenbrock integrator and
+  # the batch driver.  C_GLOBAL/C_RCONST add the optional per-cell SUN of the
+  # batch driver: Update_RCONST runs the C_RCONST block before the rate
+  # assignments (src/gen.c:2420-2435), after FunTemplate called Update_SUN.
+  cat > "$d/$mech.kpp" <<EOF
+#MODEL      $mech
+#LANGUAGE   C
+#DOUBLE     ON
+#INTEGRATOR rosenbrock
+#DRIVER     $HERE/refkpp/batch_driver
+#JACOBIAN   SPARSE_LU_ROW
+#HESSIAN    ON
+#STOICMAT   ON
+#MEX        OFF
+#INLINE C_GLOBAL
+  extern double kppref_sun_override;
+#ENDINLINE
+#INLINE C_RCONST
+  if (kppref_sun_override >= 0.0) SUN = kppref_sun_override;
+#ENDINLINE
+EOF
+  (cd "$d" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
+    echo "build_ref: kpp failed for $mech" >&2; tail -20 "$d/kpp.log" >&2; exit 1; }
+  srcs=()
+  for f in "$d/${mech}"_*.c; do
+    case "$f" in *_mex_*) ;; *) srcs+=("$f") ;; esac
+  done
+  inc=(-include "$d/${mech}_Parameters.h" -include "$d/${mech}_Global.h" -include "$d/${mech}_Sparse.h")
+  "$CC" -O -Wall -w -fPIC -shared -I"$d" "${srcs[@]}" \
+    -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}.so"
+  "$CC" -O3 -march=native -w -fPIC -shared -I"$d" "${srcs[@]}" \
+    -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}_O3.so"
+  echo "build_ref: $mech -> $d/libkppref_${mech}.so"
+done
