@@ -1,0 +1,146 @@
+/*
+ * kpp_b200.h -- C ABI of the B200 batched Rosenbrock engine for KPP
+ * mechanisms.
+ *
+ * One shared library per mechanism (libkpp_b200_<mechanism>.so), built from
+ * the mechanism's KPP files by the kppcu mechanism compiler and the
+ * hand-written sm_100a Rosenbrock kernel.  Every entry point takes plain
+ * pointers and sizes; no CUDA or torch types appear in the signatures (the
+ * stream is passed as `void *` holding a cudaStream_t, NULL = legacy default
+ * stream).
+ *
+ * Layout of batched arrays: structure of arrays with the cell index fastest,
+ * leading dimension `ld` >= ncells.  Element (species i, cell c) of VAR is
+ * var[i*ld + c].  All batched arrays are DEVICE pointers; the small control
+ * arrays ipar/rpar are HOST pointers.
+ *
+ * Return values of the entry points: KPP_B200_OK, or an error code below.
+ * Integration failures are per cell, in IERR, with the reference's codes.
+ */
+#ifndef KPP_B200_H
+#define KPP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KPP_B200_OK 0
+#define KPP_B200_EINVAL 1 /* invalid argument: size, null pointer, ld < ncells */
+#define KPP_B200_ECUDA 2  /* CUDA runtime or launch error (see last_error) */
+
+/* Per-cell integrator status codes (IERR), int/rosenbrock.c:186-199. */
+#define KPP_B200_IERR_SUCCESS 1
+#define KPP_B200_IERR_MAXSTEPS_BAD (-1)   /* improper value for max no of steps */
+#define KPP_B200_IERR_METHOD (-2)         /* Rosenbrock method not implemented */
+#define KPP_B200_IERR_HBOUNDS (-3)        /* Hmin/Hmax/Hstart must be positive */
+#define KPP_B200_IERR_FACTORS (-4)        /* FacMin/FacMax/FacRej must be positive */
+#define KPP_B200_IERR_TOLERANCES (-5)     /* improper tolerance values */
+#define KPP_B200_IERR_TOO_MANY_STEPS (-6) /* no of steps exceeds maximum bound */
+#define KPP_B200_IERR_STEP_TOO_SMALL (-7) /* step size too small */
+#define KPP_B200_IERR_SINGULAR (-8)       /* matrix is repeatedly singular */
+
+/* Mechanism description.
+ * dims[0..5] = NVAR, NFIX, NSPEC, NREACT, LU_NONZERO, NONZERO.
+ * Replaces the constants of the generated KPP_ROOT_Parameters.h
+ * (src/gen.c:2627-2720). */
+int kpp_b200_dims(int *dims);
+const char *kpp_b200_mechanism_name(void);
+/* SPC_NAMES[i] of the generated KPP_ROOT_Monitor.c; "" outside [0,NSPEC). */
+const char *kpp_b200_species_name(int i);
+/* C[0..NSPEC) after the generated Initialize() (values of #INITVALUES times
+ * CFACTOR, src/gen.c:3172-3290) and the mechanism's CFACTOR. */
+int kpp_b200_initial_values(double *c, double *cfactor);
+/* LU_IROW/LU_ICOL [LU_NONZERO] and LU_CROW/LU_DIAG [NVAR+1] of the
+ * generated KPP_ROOT_JacobianSP.c (src/gen.c:530-586). */
+int kpp_b200_lu_pattern(int *irow, int *icol, int *crow, int *diag);
+
+/* Batched Rosenbrock integration -- the drop-in for the generated INTEGRATE
+ * path: for each cell c in [0, ncells), the same computation as
+ *   Rosenbrock(VAR_c, tstart[c], tend[c], ATOL, RTOL, FunTemplate,
+ *              JacTemplate, RPAR, IPAR)            (int/rosenbrock.c:137)
+ * with the generator globals of that cell (FIX, TEMP, CFACTOR, SUN) taken
+ * from the batched inputs.  Replaces the per-cell INTEGRATE calls of
+ * drv/general.c:59-76 (int/rosenbrock.c:94-133).
+ *
+ *   var      [NVAR][ld]  in/out   VAR of every cell
+ *   fix      [NFIX][ld]  in       FIX of every cell (may be NULL if NFIX == 0)
+ *   temp     [ld]        in       TEMP
+ *   cfactor  [ld]|NULL   in       CFACTOR (NULL: the mechanism's CFACTOR)
+ *   sun      [ld]|NULL   in       SUN held constant over the call (NULL: SUN
+ *                                 from Update_SUN(TIME) at every evaluation)
+ *   tstart, tend [ld]    in       integration interval of each cell
+ *   atol, rtol           in       device arrays, [NVAR] when ipar[1] == 0,
+ *                                 else [1] (scalar tolerances)
+ *   ipar [20], rpar[20]  in       HOST arrays, the integrator controls with
+ *                                 the C indexing of int/rosenbrock.c:201-254:
+ *                                 ipar[0] autonomous, ipar[1] scalar tol,
+ *                                 ipar[2] max steps, ipar[3] method (1 Ros2,
+ *                                 2 Ros3, 3 Ros4, 4 Rodas3, 5 Rodas4);
+ *                                 rpar[0..6] Hmin, Hmax, Hstart, FacMin,
+ *                                 FacMax, FacRej, FacSafe.  Entries 10..19
+ *                                 are ignored (statistics start at zero).
+ *   hstart   [ld]|NULL   in       per-cell starting step, replaces rpar[2]
+ *                                 (warm start from the previous call's Hexit)
+ *   istatus  [8][ld]     out      IPAR[10..17]: Nfun, Njac, Nstp, Nacc, Nrej,
+ *                                 Ndec, Nsol, Nsng
+ *   rstatus  [2][ld]     out      RPAR[10..11]: Texit, Hexit
+ *   ierr     [ld]        out      return value of Rosenbrock for the cell
+ *   stream               in       cudaStream_t, asynchronous
+ */
+int kpp_b200_rosenbrock(int ncells, int ld, double *var, const double *fix,
+                        const double *temp, const double *cfactor,
+                        const double *sun, const double *tstart,
+                        const double *tend, const double *atol,
+                        const double *rtol, const int *ipar,
+                        const double *rpar, const double *hstart,
+                        int *istatus, double *rstatus, int *ierr,
+                        void *stream);
+
+/* Device workspace (bytes) that kpp_b200_rosenbrock_ws uses at most for a
+ * batch of ncells cells; 0 for mechanisms whose work arrays fit in registers.
+ * No counterpart in the reference (its integrator keeps its work arrays on
+ * the host stack, int/rosenbrock.c:470-476). */
+size_t kpp_b200_workspace_bytes(int ncells);
+
+/* kpp_b200_rosenbrock with a caller-owned device workspace instead of the
+ * library's cached one (for callers that manage device memory themselves or
+ * run concurrent batches on one stream).  A workspace smaller than
+ * kpp_b200_workspace_bytes(ncells) is used with fewer resident thread slots;
+ * one that cannot hold one block of slots is rejected with KPP_B200_EINVAL. */
+int kpp_b200_rosenbrock_ws(int ncells, int ld, double *var, const double *fix,
+                           const double *temp, const double *cfactor,
+                           const double *sun, const double *tstart,
+                           const double *tend, const double *atol,
+                           const double *rtol, const int *ipar,
+                           const double *rpar, const double *hstart,
+                           int *istatus, double *rstatus, int *ierr,
+                           void *workspace, size_t workspace_bytes,
+                           void *stream);
+
+/* Batched evaluation of the generated mechanism functions at time `time`
+ * (the same for all cells), each exactly as FunTemplate / JacTemplate /
+ * Update_RCONST compute it (int/rosenbrock.c:1257-1296, src/gen.c:642-724,
+ * 1185-1322, 2343-2473).  Any of rconst [NREACT][ld], vdot [NVAR][ld],
+ * jvs [LU_NONZERO][ld] may be NULL.  Device pointers, asynchronous. */
+int kpp_b200_fun_jac(int ncells, int ld, const double *var, const double *fix,
+                     const double *temp, const double *cfactor,
+                     const double *sun, double time, double *rconst,
+                     double *vdot, double *jvs, void *stream);
+
+/* Batched no-pivot sparse LU (KppDecomp, util/sutil.c:2-23) of jvs
+ * [LU_NONZERO][ld] in place, then one solve (KppSolve, src/gen.c:1960-2034)
+ * of x [NVAR][ld] in place when x is not NULL.  ising[ld] receives the
+ * KppDecomp return value.  Device pointers, asynchronous. */
+int kpp_b200_decomp_solve(int ncells, int ld, double *jvs, double *x,
+                          int *ising, void *stream);
+
+/* Text of the last error of this thread's last failing call. */
+const char *kpp_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KPP_B200_H */

@@ -1,0 +1,210 @@
+"""Build the native parts of kpp_b200.
+
+  1. kppcu, the KPP mechanism compiler (C++, kpp_b200/gen/), with g++.
+  2. For each mechanism in kpp_b200/mechanisms/: kppcu writes the mechanism's
+     CUDA device code (kpp_b200/_gen/<mech>.cuh), and nvcc builds the batched
+     Rosenbrock library kpp_b200/lib/libkpp_b200_<mech>.so for sm_100a.
+
+The kernel source is compiled once per part (the C ABI, and one part per
+Rosenbrock method) in parallel, then linked.  Builds are incremental: a
+stamp holding a hash of every input and flag skips up-to-date libraries.
+
+Mechanism sources (.def/.spc/.eqn) are looked up in the directory of the
+mechanism file and under $KPP_HOME/models (KPP's own layout).  Without them
+(for example on a machine that received prebuilt libraries) the existing
+libraries are kept; a missing library is an error.
+
+Usage: python -m kpp_b200.build [mech ...] [--force] [--jobs N]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+GEN_SRC = PKG / "gen"
+CSRC = PKG / "csrc"
+MECH_DIR = PKG / "mechanisms"
+BUILD = PKG / "_build"
+GEN_OUT = PKG / "_gen"
+LIB = PKG / "lib"
+INCLUDE = PKG.parent / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# --fmad=false: no FMA contraction, so the double arithmetic rounds like the
+# reference C code built without FMA (x86-64 gcc -O).
+NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-diag-suppress", "177"]
+METHOD_PARTS = [1, 2, 3, 4, 5]
+# Mechanisms at or above this LU size keep per-cell work arrays in the
+# cell-fastest global scratch layout instead of thread-local arrays.
+SCRATCH_LU_NONZERO = 200
+
+
+def default_kpp_home() -> str:
+    home = os.environ.get("KPP_HOME", "")
+    if home:
+        return home
+    for cand in ("/root/reference",):
+        if (Path(cand) / "models").is_dir():
+            return cand
+    return ""
+
+
+def nvcc() -> str:
+    path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return path
+
+
+def _hash_files(paths, extra: str = "") -> str:
+    h = hashlib.sha256(extra.encode())
+    for p in sorted(str(x) for x in paths):
+        h.update(p.encode())
+        h.update(Path(p).read_bytes())
+    return h.hexdigest()
+
+
+def _run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"command failed ({r.returncode}): {' '.join(map(str, cmd))}\n{r.stdout}")
+    return r.stdout
+
+
+def build_kppcu(force: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    exe = BUILD / "kppcu"
+    srcs = sorted(GEN_SRC.glob("*.cpp")) + sorted(GEN_SRC.glob("*.hpp"))
+    stamp = BUILD / "kppcu.stamp"
+    digest = _hash_files(srcs)
+    if not force and exe.exists() and stamp.exists() and stamp.read_text() == digest:
+        return exe
+    cxx = shutil.which("g++") or "g++"
+    _run([cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-o", str(exe)]
+         + [str(p) for p in GEN_SRC.glob("*.cpp")])
+    stamp.write_text(digest)
+    return exe
+
+
+def mechanism_sources(mech: str, kpp_home: str):
+    """Files kppcu reads for a mechanism (for the incremental-build hash)."""
+    files = [MECH_DIR / f"{mech}.kpp"]
+    if kpp_home:
+        for ext in (".def", ".spc", ".eqn"):
+            p = Path(kpp_home) / "models" / f"{mech}{ext}"
+            if p.exists():
+                files.append(p)
+        inc = Path(kpp_home) / "models" / "atoms.kpp"
+        if inc.exists():
+            files.append(inc)
+    return files
+
+
+def generate(mech: str, kpp_home: str, force: bool = False) -> Path | None:
+    """Run kppcu; returns the generated header, or None without sources."""
+    src = mechanism_sources(mech, kpp_home)
+    if len(src) < 2:
+        return None
+    GEN_OUT.mkdir(exist_ok=True)
+    exe = build_kppcu(force)
+    out = GEN_OUT / mech
+    stamp = GEN_OUT / f"{mech}.stamp"
+    digest = _hash_files(src + [exe])
+    if not force and stamp.exists() and stamp.read_text() == digest and (GEN_OUT / f"{mech}.cuh").exists():
+        return GEN_OUT / f"{mech}.cuh"
+    _run([str(exe), str(MECH_DIR / f"{mech}.kpp"), "-o", str(out), "--home", kpp_home, "--root", mech])
+    stamp.write_text(digest)
+    return GEN_OUT / f"{mech}.cuh"
+
+
+def library_path(mech: str) -> Path:
+    return LIB / f"libkpp_b200_{mech}.so"
+
+
+def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> Path:
+    LIB.mkdir(exist_ok=True)
+    objdir = BUILD / mech
+    objdir.mkdir(parents=True, exist_ok=True)
+    meta = json.loads((GEN_OUT / f"{mech}.json").read_text())
+    defines = [f'-DKPP_MECH_HEADER="{header}"']
+    if meta["lu_nonzero"] >= SCRATCH_LU_NONZERO:
+        defines.append("-DKPP_SCRATCH")
+    srcs = [CSRC / "kpp_rosenbrock.cu", CSRC / "kpp_ratelaws.cuh", header, INCLUDE / "kpp_b200.h"]
+    digest = _hash_files(srcs, " ".join(ARCH + NVCC_FLAGS + defines))
+    lib = library_path(mech)
+    stamp = objdir / "lib.stamp"
+    if not force and lib.exists() and stamp.exists() and stamp.read_text() == digest:
+        return lib
+    parts = [0] + METHOD_PARTS
+
+    def compile_part(part: int) -> Path:
+        obj = objdir / f"part{part}.o"
+        _run([nvcc()] + ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT),
+              "-c", str(CSRC / "kpp_rosenbrock.cu"), "-o", str(obj)])
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
+        objs = list(ex.map(compile_part, parts))
+    _run([nvcc()] + ARCH + ["-shared", "-o", str(lib)] + [str(o) for o in objs] + ["-lcudart"])
+    stamp.write_text(digest)
+    return lib
+
+
+def build_util(force: bool = False) -> Path:
+    """libkpp_b200_util.so: measurement helpers (FP64 peak)."""
+    LIB.mkdir(exist_ok=True)
+    BUILD.mkdir(exist_ok=True)
+    src = CSRC / "kpp_util.cu"
+    lib = LIB / "libkpp_b200_util.so"
+    flags = ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-lineinfo"]
+    stamp = BUILD / "util.stamp"
+    digest = _hash_files([src], " ".join(flags))
+    if not force and lib.exists() and stamp.exists() and stamp.read_text() == digest:
+        return lib
+    _run([nvcc()] + flags + [str(src), "-o", str(lib)])
+    stamp.write_text(digest)
+    return lib
+
+
+def all_mechanisms():
+    return sorted(p.stem for p in MECH_DIR.glob("*.kpp"))
+
+
+def build(mechs=None, force: bool = False, jobs: int | None = None, verbose: bool = True):
+    kpp_home = default_kpp_home()
+    jobs = jobs or os.cpu_count() or 4
+    mechs = mechs or all_mechanisms()
+    built = {"util": build_util(force)}
+    for mech in mechs:
+        header = generate(mech, kpp_home, force)
+        if header is None:
+            lib = library_path(mech)
+            if not lib.exists():
+                raise RuntimeError(f"no mechanism sources for {mech} (KPP_HOME={kpp_home!r}) "
+                                   f"and no prebuilt {lib}")
+            built[mech] = lib
+            continue
+        built[mech] = compile_library(mech, header, jobs, force)
+        if verbose:
+            print(f"kpp_b200.build: {mech} -> {built[mech]}", flush=True)
+    return built
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("mechs", nargs="*")
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=None)
+    a = ap.parse_args(argv)
+    build(a.mechs or None, force=a.force, jobs=a.jobs)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,863 @@
+// Batched Rosenbrock integrator for KPP mechanisms on B200 (sm_100a), and the
+// C ABI of include/kpp_b200.h.
+//
+// Built once per mechanism: KPP_MECH_HEADER names the kppcu output for it.
+//
+// Design
+//   * One grid cell per thread.  Cells are independent stiff ODE systems, so
+//     a cell never waits on another; the kernel is a plain data-parallel map.
+//   * Cell state lives in registers and thread-local memory; the batched
+//     inputs/outputs are structure-of-arrays with the cell index fastest, so
+//     every load/store of a warp is one coalesced 256-byte access.
+//   * The mechanism (rates, Fun, Jac_SP, LU, solves) is fully unrolled device
+//     code from kppcu; the method (tableau) is a template parameter, so stage
+//     loops unroll and zero coefficients disappear at compile time.
+//   * Arithmetic follows int/rosenbrock.c operation for operation; the
+//     library is built with --fmad=false so nothing is contracted into FMAs.
+//     Results then match the reference C code up to the last-ulp differences
+//     of exp/pow/log10/cos between the CUDA math library and the host libm.
+//
+// Reference: int/rosenbrock.c (Rosenbrock :137-446, RosenbrockIntegrator
+// :450-627, ros_ErrorNorm :632-659, ros_FunTimeDerivative :663-682,
+// ros_PrepareMatrix :686-737, tableaux :779-1222, Fun/JacTemplate
+// :1257-1296), util/blas.c (WAXPY skips alpha == 0, :51-82), util/sutil.c.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#include "../../include/kpp_b200.h"
+#include "kpp_ratelaws.cuh"
+#include KPP_MECH_HEADER
+
+// Translation-unit split (the build compiles this file once per part, in
+// parallel): KPP_PART 1..5 holds the kernel of Rosenbrock method 1..5 and its
+// launcher; KPP_PART 0 holds everything else and the C ABI.
+#ifndef KPP_PART
+#define KPP_PART 0
+#endif
+
+namespace kpp_b200_impl {
+
+constexpr int NVAR = KPP_NVAR;
+constexpr int NFIX = KPP_NFIX;
+constexpr int NFIX_TRUE = KPP_NFIX_TRUE;
+constexpr int NREACT = KPP_NREACT;
+constexpr int LU_NZ = KPP_LU_NONZERO;
+
+// Unit roundoff of WLAMCH('E') (util/blas.c:150-183): 2^-52.
+constexpr double kRoundoff = 2.220446049250313080847e-16;
+constexpr double kDeltaMin = 1.0e-6;  // int/rosenbrock.c:11
+
+// int/rosenbrock.c:1-3 as functions; ABS keeps the macro's unparenthesised
+// negation: ABS(a - b) of a negative difference evaluates -a - b.
+__device__ __forceinline__ double ros_max(double a, double b) { return (a >= b) ? a : b; }
+__device__ __forceinline__ double ros_min(double b, double c) { return (b < c) ? b : c; }
+__device__ __forceinline__ double ros_abs(double x) { return (x >= 0) ? x : -x; }
+__device__ __forceinline__ double ros_abs_diff(double a, double b) {
+  return ((a - b) >= 0) ? (a - b) : (-a - b);
+}
+
+// Rosenbrock method coefficients (int/rosenbrock.c:779-1222).  A and C are
+// strictly lower triangular, stored row-wise: A(i,j) = A[(i-1)(i-2)/2 + j-1].
+struct Tableau {
+  int S;
+  double A[15], C[15], M[6], E[6], Alpha[6], Gamma[6], ELO;
+  bool NewF[6];
+};
+
+__host__ __device__ constexpr Tableau make_tableau(int method) {
+  Tableau t{};
+  if (method == 1) {  // Ros2
+    const double g = 1.70710678118655;
+    t.S = 2;
+    t.A[0] = 1.0 / g;
+    t.C[0] = (-2.0) / g;
+    t.NewF[0] = true; t.NewF[1] = true;
+    t.M[0] = (3.0) / (2.0 * g); t.M[1] = (1.0) / (2.0 * g);
+    t.E[0] = 1.0 / (2.0 * g); t.E[1] = 1.0 / (2.0 * g);
+    t.ELO = 2.0;
+    t.Alpha[0] = 0.0; t.Alpha[1] = 1.0;
+    t.Gamma[0] = g; t.Gamma[1] = -g;
+  } else if (method == 2) {  // Ros3
+    t.S = 3;
+    t.A[0] = 1.0; t.A[1] = 1.0; t.A[2] = 0.0;
+    t.C[0] = -1.0156171083877702091975600115545;
+    t.C[1] = 4.0759956452537699824805835358067;
+    t.C[2] = 9.2076794298330791242156818474003;
+    t.NewF[0] = true; t.NewF[1] = true; t.NewF[2] = false;
+    t.M[0] = 1.0;
+    t.M[1] = 6.1697947043828245592553615689730;
+    t.M[2] = -0.4277225654321857332623837380651;
+    t.E[0] = 0.5;
+    t.E[1] = -2.9079558716805469821718236208017;
+    t.E[2] = 0.2235406989781156962736090927619;
+    t.ELO = 3.0;
+    t.Alpha[0] = 0.0;
+    t.Alpha[1] = 0.43586652150845899941601945119356;
+    t.Alpha[2] = 0.43586652150845899941601945119356;
+    t.Gamma[0] = 0.43586652150845899941601945119356;
+    t.Gamma[1] = 0.24291996454816804366592249683314;
+    t.Gamma[2] = 2.1851380027664058511513169485832;
+  } else if (method == 3) {  // Ros4
+    t.S = 4;
+    t.A[0] = 0.2000000000000000e+01;
+    t.A[1] = 0.1867943637803922e+01;
+    t.A[2] = 0.2344449711399156;
+    t.A[3] = t.A[1]; t.A[4] = t.A[2]; t.A[5] = 0.0;
+    t.C[0] = -0.7137615036412310e+01;
+    t.C[1] = 0.2580708087951457e+01;
+    t.C[2] = 0.6515950076447975;
+    t.C[3] = -0.2137148994382534e+01;
+    t.C[4] = -0.3214669691237626;
+    t.C[5] = -0.6949742501781779;
+    t.NewF[0] = true; t.NewF[1] = true; t.NewF[2] = true; t.NewF[3] = false;
+    t.M[0] = 0.2255570073418735e+01;
+    t.M[1] = 0.2870493262186792;
+    t.M[2] = 0.4353179431840180;
+    t.M[3] = 0.1093502252409163e+01;
+    t.E[0] = -0.2815431932141155;
+    t.E[1] = -0.7276199124938920e-01;
+    t.E[2] = -0.1082196201495311;
+    t.E[3] = -0.1093502252409163e+01;
+    t.ELO = 4.0;
+    t.Alpha[0] = 0.0;
+    t.Alpha[1] = 0.1145640000000000e+01;
+    t.Alpha[2] = 0.6552168638155900;
+    t.Alpha[3] = t.Alpha[2];
+    t.Gamma[0] = 0.5728200000000000;
+    t.Gamma[1] = -0.1769193891319233e+01;
+    t.Gamma[2] = 0.7592633437920482;
+    t.Gamma[3] = -0.1049021087100450;
+  } else if (method == 4) {  // Rodas3
+    t.S = 4;
+    t.A[0] = 0.0; t.A[1] = 2.0; t.A[2] = 0.0; t.A[3] = 2.0; t.A[4] = 0.0; t.A[5] = 1.0;
+    t.C[0] = 4.0; t.C[1] = 1.0; t.C[2] = -1.0; t.C[3] = 1.0; t.C[4] = -1.0;
+    t.C[5] = -2.66666666666667;
+    t.NewF[0] = true; t.NewF[1] = false; t.NewF[2] = true; t.NewF[3] = true;
+    t.M[0] = 2.0; t.M[1] = 0.0; t.M[2] = 1.0; t.M[3] = 1.0;
+    t.E[0] = 0.0; t.E[1] = 0.0; t.E[2] = 0.0; t.E[3] = 1.0;
+    t.ELO = 3.0;
+    t.Alpha[0] = 0.0; t.Alpha[1] = 0.0; t.Alpha[2] = 1.0; t.Alpha[3] = 1.0;
+    t.Gamma[0] = 0.5; t.Gamma[1] = 1.5; t.Gamma[2] = 0.0; t.Gamma[3] = 0.0;
+  } else if (method == 5) {  // Rodas4
+    t.S = 6;
+    t.Alpha[0] = 0.000; t.Alpha[1] = 0.386; t.Alpha[2] = 0.210;
+    t.Alpha[3] = 0.630; t.Alpha[4] = 1.000; t.Alpha[5] = 1.000;
+    t.Gamma[0] = 0.2500000000000000; t.Gamma[1] = -0.1043000000000000;
+    t.Gamma[2] = 0.1035000000000000; t.Gamma[3] = -0.3620000000000023e-01;
+    t.Gamma[4] = 0.0; t.Gamma[5] = 0.0;
+    t.A[0] = 0.1544000000000000e+01; t.A[1] = 0.9466785280815826;
+    t.A[2] = 0.2557011698983284; t.A[3] = 0.3314825187068521e+01;
+    t.A[4] = 0.2896124015972201e+01; t.A[5] = 0.9986419139977817;
+    t.A[6] = 0.1221224509226641e+01; t.A[7] = 0.6019134481288629e+01;
+    t.A[8] = 0.1253708332932087e+02; t.A[9] = -0.6878860361058950;
+    t.A[10] = t.A[6]; t.A[11] = t.A[7]; t.A[12] = t.A[8]; t.A[13] = t.A[9];
+    t.A[14] = 1.0;
+    t.C[0] = -0.5668800000000000e+01; t.C[1] = -0.2430093356833875e+01;
+    t.C[2] = -0.2063599157091915; t.C[3] = -0.1073529058151375;
+    t.C[4] = -0.9594562251023355e+01; t.C[5] = -0.2047028614809616e+02;
+    t.C[6] = 0.7496443313967647e+01; t.C[7] = -0.1024680431464352e+02;
+    t.C[8] = -0.3399990352819905e+02; t.C[9] = 0.1170890893206160e+02;
+    t.C[10] = 0.8083246795921522e+01; t.C[11] = -0.7981132988064893e+01;
+    t.C[12] = -0.3152159432874371e+02; t.C[13] = 0.1631930543123136e+02;
+    t.C[14] = -0.6058818238834054e+01;
+    t.M[0] = t.A[6]; t.M[1] = t.A[7]; t.M[2] = t.A[8]; t.M[3] = t.A[9];
+    t.M[4] = 1.0; t.M[5] = 1.0;
+    t.E[5] = 1.0;
+    for (int i = 0; i < 6; i++) t.NewF[i] = true;
+    t.ELO = 4.0;
+  }
+  return t;
+}
+
+// Everything one launch needs.  Passed by value (kernel parameter space).
+struct LaunchArgs {
+  int ncells, ld;
+  double* var;
+  const double* fix;
+  const double* temp;
+  const double* cfactor;
+  const double* sun;
+  const double* tstart;
+  const double* tend;
+  const double* atol;
+  const double* rtol;
+  const double* hstart;
+  int* istatus;
+  double* rstatus;
+  int* ierr;
+  double* scratch;  // work arrays of every thread slot (scratch layout), or null
+  long nslots;      // thread slots of the grid = stride of the scratch arrays
+  int ipar[20];
+  double rpar[20];
+};
+
+struct Stats {
+  int nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng;
+};
+
+// A per-cell array of a thread slot inside the scratch buffer: element i at
+// p[i * s].  Consecutive slots are consecutive doubles, so a warp touching
+// the same element of 32 cells issues one coalesced 256-byte access.
+struct Strided {
+  double* p;
+  long s;
+  __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * s]; }
+};
+
+// Doubles of work storage one thread slot needs in the scratch layout.
+constexpr int kMaxStages = 6;
+constexpr long kScratchPerSlot = (long)LU_NZ + (long)kMaxStages * NVAR + 6L * NVAR +
+                                 2L * NREACT + KPP_NJAC_TMP;
+
+#if defined(KPP_SCRATCH)
+// Large mechanisms: every per-cell work array lives in the scratch buffer.
+struct Work {
+  Strided y, ynew, fcn0, fcn, dfdt, yerr, jvs, rconst, a, b;
+  Strided k[kMaxStages];
+  __device__ __forceinline__ Work(double* base, long nslots, long slot) {
+    long off = 0;
+    auto take = [&](long n) {
+      Strided v{base + off * nslots + slot, nslots};
+      off += n;
+      return v;
+    };
+    y = take(NVAR); ynew = take(NVAR); fcn0 = take(NVAR); fcn = take(NVAR);
+    dfdt = take(NVAR); yerr = take(NVAR); jvs = take(LU_NZ);
+    rconst = take(NREACT); a = take(NREACT); b = take(KPP_NJAC_TMP);
+    for (int s = 0; s < kMaxStages; s++) k[s] = take(NVAR);
+  }
+};
+#else
+// Small mechanisms: work arrays are thread-local (registers).
+struct Work {
+  double y[NVAR], ynew[NVAR], fcn0[NVAR], fcn[NVAR], dfdt[NVAR], yerr[NVAR];
+  double jvs[LU_NZ], rconst[NREACT > 0 ? NREACT : 1], a[NREACT > 0 ? NREACT : 1];
+  double b[KPP_NJAC_TMP];
+  double k[kMaxStages][NVAR];
+  __device__ __forceinline__ Work(double*, long, long) {}
+};
+#endif
+
+// The environment one cell's rate constants see (the generator's globals).
+struct CellEnv {
+  double temp, cfactor, sun_fixed;  // sun_fixed < 0: SUN from Update_SUN(TIME)
+  double fix[NFIX];
+};
+
+__device__ __forceinline__ double cell_sun(const CellEnv& env, double t) {
+  return env.sun_fixed >= 0.0 ? env.sun_fixed : kpp_update_sun(t);
+}
+
+// Rate constants that stay fixed for the whole integration of a cell: those
+// depending only on TEMP/CFACTOR, and the SUN-dependent ones when SUN is
+// given per cell.
+template <class W>
+__device__ __forceinline__ void rates_once(const CellEnv& env, double t, W& w) {
+  kpp_rconst_static(w.rconst, t, env.temp, env.cfactor, 0.0, w.y, env.fix);
+  if (env.sun_fixed >= 0.0)
+    kpp_rconst_sun(w.rconst, t, env.temp, env.cfactor, env.sun_fixed, w.y, env.fix);
+}
+
+// Rate constants that change with the time of an evaluation.  The reference
+// recomputes all of them at every FunTemplate/JacTemplate call
+// (int/rosenbrock.c:1267-1268,1289-1290); recomputing only those whose inputs
+// changed gives the same values.
+template <class W>
+__device__ __forceinline__ bool rates_vary(const CellEnv& env) {
+  return KPP_RATES_DYNAMIC > 0 || (KPP_RATES_SUN > 0 && env.sun_fixed < 0.0);
+}
+template <class W>
+__device__ __forceinline__ void rates_at(const CellEnv& env, double t, W& w) {
+  if (KPP_RATES_SUN > 0 && env.sun_fixed < 0.0)
+    kpp_rconst_sun(w.rconst, t, env.temp, env.cfactor, kpp_update_sun(t), w.y, env.fix);
+  if (KPP_RATES_DYNAMIC > 0)
+    kpp_rconst_dynamic(w.rconst, t, env.temp, env.cfactor, cell_sun(env, t), w.y, env.fix);
+}
+
+// WAXPY (util/blas.c:51-82): y <- y + alpha*x, nothing when alpha == 0.
+template <class TX, class TY>
+__device__ __forceinline__ void axpy(double alpha, const TX& x, TY& y) {
+  if (alpha == 0.0) return;
+#pragma unroll 4
+  for (int i = 0; i < NVAR; i++) y[i] = y[i] + alpha * x[i];
+}
+
+template <class TX, class TY>
+__device__ __forceinline__ void copy(const TX& x, TY& y) {
+#pragma unroll 4
+  for (int i = 0; i < NVAR; i++) y[i] = x[i];
+}
+
+// ros_ErrorNorm (int/rosenbrock.c:632-659); SQRT(x) of the reference is
+// pow(x, 0.5), computed here as the correctly rounded sqrt.
+template <class TA, class TB, class TC>
+__device__ __forceinline__ double error_norm(const TA& y, const TB& ynew, const TC& yerr,
+                                             const double* atol, const double* rtol,
+                                             bool vectortol) {
+  double err = 0.0;
+  const double a0 = atol[0], r0 = rtol[0];
+#pragma unroll 4
+  for (int i = 0; i < NVAR; i++) {
+    double ymax = ros_max(ros_abs(y[i]), ros_abs(ynew[i]));
+    double scale = vectortol ? (atol[i] + rtol[i] * ymax) : (a0 + r0 * ymax);
+    err = err + (yerr[i] * yerr[i]) / (scale * scale);
+  }
+  return sqrt(err / (double)NVAR);
+}
+
+// ros_PrepareMatrix (int/rosenbrock.c:686-737): Ghimj = -Jac0 + 1/(H*gam) I,
+// LU factorise; halve H on a singular factorisation, give up after 5.
+// Instead of keeping Jac0 the negated Jacobian is evaluated straight into
+// Ghimj at time t (rates at t are in w.rconst); a second attempt evaluates it
+// again from the same inputs, which reproduces Jac0 exactly.
+template <class W>
+__device__ __forceinline__ bool prepare_matrix(const CellEnv& env, double t, double& h,
+                                               int direction, double gam, W& w, Stats& st) {
+  int nconsecutive = 0;
+  for (;;) {
+    kpp_jac_sp<true>(w.y, env.fix, w.rconst, w.jvs, w.b);
+    double ghinv = 1.0 / (direction * h * gam);
+    kpp_add_diagonal(w.jvs, ghinv);
+    int ising = kpp_decomp(w.jvs);
+    st.ndec++;
+    if (ising == 0) return false;
+    st.nsng++;
+    nconsecutive++;
+    if (nconsecutive <= 5) h = h * 0.5;
+    else return true;
+  }
+}
+
+// RosenbrockIntegrator (int/rosenbrock.c:450-627) for one cell; w.y holds
+// the cell state in and out.
+template <int METHOD, class W>
+__device__ int integrate_cell(const CellEnv& env, W& w, double tstart, double tend,
+                              const double* atol, const double* rtol, bool autonomous,
+                              bool vectortol, int max_no_steps, double hmin, double hmax,
+                              double hstart, double facmin, double facmax, double facrej,
+                              double facsafe, double& texit, double& hexit, Stats& st) {
+  constexpr Tableau tab = make_tableau(METHOD);
+  constexpr int S = tab.S;
+
+  double t = tstart;
+  hexit = 0.0;
+  double h = ros_min(hstart, hmax);
+  if (ros_abs(h) <= 10.0 * kRoundoff) h = kDeltaMin;
+  const int direction = (tend >= tstart) ? +1 : -1;
+  bool reject_last = false, reject_more = false;
+  const bool varying = rates_vary<W>(env);
+  rates_once(env, t, w);
+
+  while (((direction > 0) && ((t - tend) + kRoundoff <= 0.0)) ||
+         ((direction < 0) && ((tend - t) + kRoundoff <= 0.0))) {
+    if (st.nstp > max_no_steps) { texit = t; return KPP_B200_IERR_TOO_MANY_STEPS; }
+    if (((t + 0.1 * h) == t) || (h <= kRoundoff)) { texit = t; return KPP_B200_IERR_STEP_TOO_SMALL; }
+    hexit = h;
+    h = ros_min(h, ros_abs_diff(tend, t));
+
+    // FunTemplate(T, Y, Fcn0)
+    rates_at(env, t, w);
+    kpp_fun(w.y, env.fix, w.rconst, w.fcn0, w.a);
+    st.nfun++;
+    if (!autonomous) {
+      // ros_FunTimeDerivative (:663-682): dFdT = (Fun(T+Delta) - Fcn0)/Delta
+      double delta = sqrt(kRoundoff) * ros_max(kDeltaMin, ros_abs(t));
+      if (varying) {
+        rates_at(env, t + delta, w);
+        kpp_fun(w.y, env.fix, w.rconst, w.dfdt, w.a);
+        rates_at(env, t, w);  // JacTemplate(T) below sees the rates at T
+      } else {
+        // Fun(T+Delta) would see the same rates and state: Fcn0 again
+        copy(w.fcn0, w.dfdt);
+      }
+      st.nfun++;
+      axpy(-1.0, w.fcn0, w.dfdt);
+      double inv = 1.0 / delta;
+      if (inv != 1.0) {
+#pragma unroll 4
+        for (int i = 0; i < NVAR; i++) w.dfdt[i] = inv * w.dfdt[i];
+      }
+    }
+    st.njac++;  // JacTemplate(T, Y, Jac0), evaluated inside prepare_matrix
+
+    bool retry = false;
+    for (;;) {  // until the step is accepted
+      if (retry && varying) rates_at(env, t, w);  // stages moved the rates to Tau
+      retry = true;
+      if (prepare_matrix(env, t, h, direction, tab.Gamma[0], w, st)) {
+        texit = t;
+        return KPP_B200_IERR_SINGULAR;
+      }
+#pragma unroll
+      for (int s = 0; s < S; s++) {
+        if (s == 0) {
+          copy(w.fcn0, w.fcn);
+        } else if (tab.NewF[s]) {
+          copy(w.y, w.ynew);
+#pragma unroll
+          for (int j = 0; j < s; j++) axpy(tab.A[s * (s - 1) / 2 + j], w.k[j], w.ynew);
+          double tau = t + tab.Alpha[s] * direction * h;
+          if (varying) rates_at(env, tau, w);
+          kpp_fun(w.ynew, env.fix, w.rconst, w.fcn, w.a);
+          st.nfun++;
+        }
+        copy(w.fcn, w.k[s]);
+#pragma unroll
+        for (int j = 0; j < s; j++) {
+          double hc = tab.C[s * (s - 1) / 2 + j] / (direction * h);
+          axpy(hc, w.k[j], w.k[s]);
+        }
+        if ((!autonomous) && (tab.Gamma[s] != 0.0)) {
+          double hg = direction * h * tab.Gamma[s];
+          axpy(hg, w.dfdt, w.k[s]);
+        }
+        kpp_solve(w.jvs, w.k[s]);
+        st.nsol++;
+      }
+
+      copy(w.y, w.ynew);
+#pragma unroll
+      for (int j = 0; j < S; j++) axpy(tab.M[j], w.k[j], w.ynew);
+#pragma unroll 4
+      for (int i = 0; i < NVAR; i++) w.yerr[i] = 0.0;
+#pragma unroll
+      for (int j = 0; j < S; j++) axpy(tab.E[j], w.k[j], w.yerr);
+      double err = error_norm(w.y, w.ynew, w.yerr, atol, rtol, vectortol);
+
+      double fac = ros_min(facmax, ros_max(facmin, facsafe / pow(err, 1.0 / tab.ELO)));
+      double hnew = h * fac;
+
+      st.nstp++;
+      if ((err <= 1.0) || (h <= hmin)) {
+        st.nacc++;
+        copy(w.ynew, w.y);
+        t += direction * h;
+        hnew = ros_max(hmin, ros_min(hnew, hmax));
+        if (reject_last) hnew = ros_min(hnew, h);
+        reject_last = false;
+        reject_more = false;
+        h = hnew;
+        break;
+      } else {
+        if (st.nacc >= 1) st.nrej++;
+        if (reject_more) hnew = h * facrej;
+        reject_more = reject_last;
+        reject_last = true;
+        h = hnew;
+      }
+    }
+  }
+  texit = t;
+  return KPP_B200_IERR_SUCCESS;
+}
+
+// Rosenbrock (int/rosenbrock.c:137-446): validation and defaults, then the
+// integrator.  Returns IERR; fills stats/texit/hexit like IPAR/RPAR[10..].
+template <int METHOD, class W>
+__device__ int rosenbrock_cell(const CellEnv& env, W& w, double tstart, double tend,
+                               const double* atol, const double* rtol, const LaunchArgs& a,
+                               double rpar2, Stats& st, double& texit, double& hexit) {
+  const int* ipar = a.ipar;
+  const double* rpar = a.rpar;
+  bool autonomous = !(ipar[0] == 0);
+  bool vectortol = (ipar[1] == 0);
+  int uplimtol = vectortol ? NVAR : 1;
+  int max_no_steps = (ipar[2] == 0) ? 100000 : ipar[2];
+  if (max_no_steps < 0) return KPP_B200_IERR_MAXSTEPS_BAD;
+  if ((ipar[3] < 1) || (ipar[3] > 5)) return KPP_B200_IERR_METHOD;
+  double hmin = rpar[0];
+  if (rpar[0] < 0.0) return KPP_B200_IERR_HBOUNDS;
+  double hmax = (rpar[1] == 0.0) ? ros_abs_diff(tend, tstart)
+                                 : ros_min(ros_abs(rpar[1]), ros_abs_diff(tend, tstart));
+  if (rpar[1] < 0.0) return KPP_B200_IERR_HBOUNDS;
+  double hstart = (rpar2 == 0.0) ? ros_max(hmin, kDeltaMin)
+                                 : ros_min(ros_abs(rpar2), ros_abs_diff(tend, tstart));
+  if (rpar2 < 0.0) return KPP_B200_IERR_HBOUNDS;
+  double facmin = (rpar[3] == 0.0) ? 0.2 : rpar[3];
+  if (rpar[3] < 0.0) return KPP_B200_IERR_FACTORS;
+  double facmax = (rpar[4] == 0.0) ? 6.0 : rpar[4];
+  if (rpar[4] < 0.0) return KPP_B200_IERR_FACTORS;
+  double facrej = (rpar[5] == 0.0) ? 0.1 : rpar[5];
+  if (rpar[5] < 0.0) return KPP_B200_IERR_FACTORS;
+  double facsafe = (rpar[6] == 0.0) ? 0.9 : rpar[6];
+  if (rpar[6] < 0.0) return KPP_B200_IERR_FACTORS;
+  for (int i = 0; i < uplimtol; i++)
+    if ((atol[i] <= 0.0) || (rtol[i] <= 10.0 * kRoundoff) || (rtol[i] >= 1.0))
+      return KPP_B200_IERR_TOLERANCES;
+  return integrate_cell<METHOD>(env, w, tstart, tend, atol, rtol, autonomous, vectortol,
+                                max_no_steps, hmin, hmax, hstart, facmin, facmax, facrej,
+                                facsafe, texit, hexit, st);
+}
+
+__device__ __forceinline__ void load_env(CellEnv& env, const double* temp, const double* cfactor,
+                                         const double* sun, const double* fix, long ld, int cell) {
+  env.temp = temp[cell];
+  env.cfactor = cfactor ? cfactor[cell] : KPP_CFACTOR;
+  env.sun_fixed = sun ? sun[cell] : -1.0;
+#pragma unroll
+  for (int i = 0; i < NFIX; i++) env.fix[i] = (i < NFIX_TRUE) ? fix[i * ld + cell] : 0.0;
+}
+
+// Text of the last error of the calling thread (defined in part 0).
+extern thread_local char g_last_error[512];
+
+inline int fail(int code, const char* msg) {
+  std::snprintf(g_last_error, sizeof g_last_error, "%s", msg);
+  return code;
+}
+
+inline int cuda_fail(const char* what, cudaError_t e) {
+  std::snprintf(g_last_error, sizeof g_last_error, "%s: %s", what, cudaGetErrorString(e));
+  return KPP_B200_ECUDA;
+}
+
+inline int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? KPP_B200_OK : cuda_fail(what, e);
+}
+
+constexpr int kBlock = 128;
+
+// Launcher and occupancy of the kernel of method M, defined in part M.
+template <int M>
+int launch_method(LaunchArgs& a, int grid, cudaStream_t s);
+template <int M>
+int occupancy_method();
+
+#if KPP_PART >= 1
+// One thread slot integrates cells slot, slot + nslots, ... (grid-stride).
+template <int METHOD>
+__global__ void __launch_bounds__(128) rosenbrock_kernel(const LaunchArgs a) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long ld = a.ld;
+  Work w(a.scratch, a.nslots, slot);
+  for (long c = slot; c < a.ncells; c += a.nslots) {
+    const int cell = (int)c;
+    CellEnv env;
+    load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
+#pragma unroll 4
+    for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
+
+    Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
+    double texit = 0.0, hexit = 0.0;
+    const double rpar2 = a.hstart ? a.hstart[cell] : a.rpar[2];
+    int ierr = rosenbrock_cell<METHOD>(env, w, a.tstart[cell], a.tend[cell], a.atol, a.rtol, a,
+                                       rpar2, st, texit, hexit);
+
+    // y is untouched when the controls were rejected (IERR -1..-5); the
+    // statistics and Texit/Hexit are then zero, as IPAR/RPAR[10..] stay.
+    a.ierr[cell] = ierr;
+#pragma unroll 4
+    for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+    const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
+#pragma unroll
+    for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
+    a.rstatus[cell] = texit;
+    a.rstatus[ld + cell] = hexit;
+  }
+}
+
+
+template <int M>
+int launch_method(LaunchArgs& a, int grid, cudaStream_t s) {
+  rosenbrock_kernel<M><<<grid, kBlock, 0, s>>>(a);
+  return check_launch("rosenbrock_kernel");
+}
+
+template <int M>
+int occupancy_method() {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rosenbrock_kernel<M>, kBlock, 0) !=
+      cudaSuccess)
+    per_sm = 1;
+  return per_sm;
+}
+
+template int launch_method<KPP_PART>(LaunchArgs&, int, cudaStream_t);
+template int occupancy_method<KPP_PART>();
+
+#else  // KPP_PART == 0
+
+thread_local char g_last_error[512] = "";
+
+// Per-cell evaluation of the mechanism functions (test and tooling entry).
+struct EvalArgs {
+  int ncells, ld;
+  const double* var;
+  const double* fix;
+  const double* temp;
+  const double* cfactor;
+  const double* sun;
+  double time;
+  double* rconst;
+  double* vdot;
+  double* jvs;
+  double* scratch;
+  long nslots;
+};
+
+__global__ void __launch_bounds__(128) fun_jac_kernel(const EvalArgs a) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long ld = a.ld;
+  Work w(a.scratch, a.nslots, slot);
+  for (long c = slot; c < a.ncells; c += a.nslots) {
+    const int cell = (int)c;
+    CellEnv env;
+    load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
+    for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
+    kpp_update_rconst(w.rconst, a.time, env.temp, env.cfactor, cell_sun(env, a.time), w.y,
+                      env.fix);
+    if (a.rconst)
+      for (int i = 0; i < NREACT; i++) a.rconst[i * ld + cell] = w.rconst[i];
+    if (a.vdot) {
+      kpp_fun(w.y, env.fix, w.rconst, w.fcn, w.a);
+      for (int i = 0; i < NVAR; i++) a.vdot[i * ld + cell] = w.fcn[i];
+    }
+    if (a.jvs) {
+      kpp_jac_sp<false>(w.y, env.fix, w.rconst, w.jvs, w.b);
+      for (int i = 0; i < LU_NZ; i++) a.jvs[i * ld + cell] = w.jvs[i];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) decomp_solve_kernel(int ncells, int ld, double* jvs_g,
+                                                           double* x_g, int* ising) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= ncells) return;
+  Strided jvs{jvs_g + cell, ld};
+  ising[cell] = kpp_decomp(jvs);
+  if (x_g) {
+    Strided x{x_g + cell, ld};
+    kpp_solve(jvs, x);
+  }
+}
+
+
+
+#if defined(KPP_SCRATCH)
+constexpr bool kUsesScratch = true;
+#else
+constexpr bool kUsesScratch = false;
+#endif
+
+// Thread slots a launch over ncells cells uses: one per cell, at most as many
+// as the device keeps resident (the rest of the cells are picked up by the
+// grid-stride loop), in whole blocks.
+long slots_for(int ncells) {
+  static std::mutex mu;
+  static std::map<int, long> resident;  // device -> resident threads
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return kBlock;
+  long res;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = resident.find(dev);
+    if (it == resident.end()) {
+      int sms = 1, per_sm = 1;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      per_sm = occupancy_method<4>();
+      if (per_sm < 1) per_sm = 1;
+      it = resident.emplace(dev, (long)sms * per_sm * kBlock).first;
+    }
+    res = it->second;
+  }
+  long want = ((long)ncells + kBlock - 1) / kBlock * kBlock;
+  return want < res ? want : res;
+}
+
+size_t scratch_bytes(long nslots) {
+  return kUsesScratch ? (size_t)kScratchPerSlot * (size_t)nslots * sizeof(double) : 0;
+}
+
+// Library-managed work buffers, one per (device, stream), grown on demand and
+// kept until exit.  Growing calls cudaMalloc, which synchronises the device.
+int cached_scratch(cudaStream_t stream, size_t bytes, double** out) {
+  static std::mutex mu;
+  static std::map<std::pair<int, cudaStream_t>, std::pair<void*, size_t>> cache;
+  *out = nullptr;
+  if (bytes == 0) return KPP_B200_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  std::lock_guard<std::mutex> lock(mu);
+  auto& entry = cache[{dev, stream}];
+  if (entry.second < bytes) {
+    if (entry.first) {
+      cudaStreamSynchronize(stream);
+      cudaFree(entry.first);
+      entry = {nullptr, 0};
+    }
+    void* p = nullptr;
+    e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return cuda_fail("cudaMalloc(workspace)", e);
+    entry = {p, bytes};
+  }
+  *out = (double*)entry.first;
+  return KPP_B200_OK;
+}
+
+int launch_rosenbrock(LaunchArgs& a, cudaStream_t s) {
+  const int grid = (int)(a.nslots / kBlock);
+  // Invalid methods are reported per cell by the validation in
+  // rosenbrock_cell (IERR = -2); any valid instance does that.
+  switch (a.ipar[3]) {
+    case 1: return launch_method<1>(a, grid, s);
+    case 2: return launch_method<2>(a, grid, s);
+    case 3: return launch_method<3>(a, grid, s);
+    case 5: return launch_method<5>(a, grid, s);
+    default: return launch_method<4>(a, grid, s);
+  }
+}
+
+int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
+              const double* temp, const double* cfactor, const double* sun,
+              const double* tstart, const double* tend, const double* atol, const double* rtol,
+              const int* ipar, const double* rpar, const double* hstart, int* istatus,
+              double* rstatus, int* ierr) {
+  if (ncells < 0 || ld < ncells) return fail(KPP_B200_EINVAL, "need 0 <= ncells <= ld");
+  if (ncells > 0 && (!var || !temp || !tstart || !tend || !atol || !rtol || !ipar || !rpar ||
+                     !istatus || !rstatus || !ierr || (KPP_NFIX_TRUE > 0 && !fix)))
+    return fail(KPP_B200_EINVAL, "null argument");
+  a.ncells = ncells;
+  a.ld = ld;
+  a.var = var;
+  a.fix = fix;
+  a.temp = temp;
+  a.cfactor = cfactor;
+  a.sun = sun;
+  a.tstart = tstart;
+  a.tend = tend;
+  a.atol = atol;
+  a.rtol = rtol;
+  a.hstart = hstart;
+  a.istatus = istatus;
+  a.rstatus = rstatus;
+  a.ierr = ierr;
+  a.scratch = nullptr;
+  a.nslots = 0;
+  if (ipar) std::memcpy(a.ipar, ipar, sizeof a.ipar);
+  if (rpar) std::memcpy(a.rpar, rpar, sizeof a.rpar);
+  return KPP_B200_OK;
+}
+
+#endif  // KPP_PART
+
+}  // namespace kpp_b200_impl
+
+#if KPP_PART == 0
+using namespace kpp_b200_impl;
+
+extern "C" {
+
+int kpp_b200_dims(int* dims) {
+  if (!dims) return fail(KPP_B200_EINVAL, "dims is NULL");
+  dims[0] = KPP_NVAR;
+  dims[1] = KPP_NFIX_TRUE;
+  dims[2] = KPP_NSPEC;
+  dims[3] = KPP_NREACT;
+  dims[4] = KPP_LU_NONZERO;
+  dims[5] = KPP_NONZERO;
+  return KPP_B200_OK;
+}
+
+const char* kpp_b200_mechanism_name(void) { return KPP_MECH_NAME; }
+
+const char* kpp_b200_species_name(int i) {
+  return (i >= 0 && i < KPP_NSPEC) ? kpp_mech::kSpeciesNames[i] : "";
+}
+
+int kpp_b200_initial_values(double* c, double* cfactor) {
+  if (!c || !cfactor) return fail(KPP_B200_EINVAL, "null argument");
+  for (int i = 0; i < KPP_NSPEC; i++) c[i] = kpp_mech::kInitialValues[i] * KPP_CFACTOR;
+  *cfactor = KPP_CFACTOR;
+  return KPP_B200_OK;
+}
+
+int kpp_b200_lu_pattern(int* irow, int* icol, int* crow, int* diag) {
+  if (!irow || !icol || !crow || !diag) return fail(KPP_B200_EINVAL, "null argument");
+  for (int i = 0; i < KPP_LU_NONZERO; i++) {
+    irow[i] = kpp_mech::kLuIRow[i];
+    icol[i] = kpp_mech::kLuICol[i];
+  }
+  for (int i = 0; i <= KPP_NVAR; i++) {
+    crow[i] = kpp_mech::kLuCRow[i];
+    diag[i] = kpp_mech::kLuDiag[i];
+  }
+  return KPP_B200_OK;
+}
+
+int kpp_b200_rosenbrock(int ncells, int ld, double* var, const double* fix, const double* temp,
+                        const double* cfactor, const double* sun, const double* tstart,
+                        const double* tend, const double* atol, const double* rtol,
+                        const int* ipar, const double* rpar, const double* hstart,
+                        int* istatus, double* rstatus, int* ierr, void* stream) {
+  LaunchArgs a;
+  int rc = fill_args(a, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, ipar,
+                     rpar, hstart, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  a.nslots = slots_for(ncells);
+  rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+  if (rc != KPP_B200_OK) return rc;
+  return launch_rosenbrock(a, s);
+}
+
+size_t kpp_b200_workspace_bytes(int ncells) {
+  return ncells > 0 ? scratch_bytes(slots_for(ncells)) : 0;
+}
+
+int kpp_b200_rosenbrock_ws(int ncells, int ld, double* var, const double* fix, const double* temp,
+                           const double* cfactor, const double* sun, const double* tstart,
+                           const double* tend, const double* atol, const double* rtol,
+                           const int* ipar, const double* rpar, const double* hstart,
+                           int* istatus, double* rstatus, int* ierr, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  LaunchArgs a;
+  int rc = fill_args(a, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, ipar,
+                     rpar, hstart, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  a.nslots = slots_for(ncells);
+  if (kUsesScratch) {
+    long fit = (long)(workspace_bytes / ((size_t)kScratchPerSlot * sizeof(double)));
+    fit = fit / kBlock * kBlock;
+    if (!workspace || fit < kBlock)
+      return fail(KPP_B200_EINVAL, "workspace smaller than one block of thread slots");
+    if (fit < a.nslots) a.nslots = fit;
+    a.scratch = (double*)workspace;
+  }
+  return launch_rosenbrock(a, (cudaStream_t)stream);
+}
+
+int kpp_b200_fun_jac(int ncells, int ld, const double* var, const double* fix,
+                     const double* temp, const double* cfactor, const double* sun, double time,
+                     double* rconst, double* vdot, double* jvs, void* stream) {
+  if (ncells < 0 || ld < ncells) return fail(KPP_B200_EINVAL, "need 0 <= ncells <= ld");
+  if (ncells == 0) return KPP_B200_OK;
+  if (!var || !temp || (KPP_NFIX_TRUE > 0 && !fix)) return fail(KPP_B200_EINVAL, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  EvalArgs a{ncells, ld, var, fix, temp, cfactor, sun, time, rconst, vdot, jvs, nullptr, 0};
+  a.nslots = slots_for(ncells);
+  int rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+  if (rc != KPP_B200_OK) return rc;
+  fun_jac_kernel<<<(int)(a.nslots / kBlock), kBlock, 0, s>>>(a);
+  return check_launch("fun_jac_kernel");
+}
+
+int kpp_b200_decomp_solve(int ncells, int ld, double* jvs, double* x, int* ising, void* stream) {
+  if (ncells < 0 || ld < ncells) return fail(KPP_B200_EINVAL, "need 0 <= ncells <= ld");
+  if (ncells == 0) return KPP_B200_OK;
+  if (!jvs || !ising) return fail(KPP_B200_EINVAL, "null argument");
+  decomp_solve_kernel<<<(ncells + kBlock - 1) / kBlock, kBlock, 0, (cudaStream_t)stream>>>(
+      ncells, ld, jvs, x, ising);
+  return check_launch("decomp_solve_kernel");
+}
+
+const char* kpp_b200_last_error(void) { return g_last_error; }
+
+}  // extern "C"
+
+#endif  // KPP_PART == 0

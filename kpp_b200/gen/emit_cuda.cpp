@@ -1,0 +1,500 @@
+// kppcu CUDA emitter.
+//
+// Writes one header, <prefix>.cuh, holding the mechanism as sm_100a device
+// code plus the host-side tables the C-ABI exports:
+//   kpp_update_rconst  rate constants (the mechanism's rate expressions,
+//                      src/gen.c:2343-2473, with the rate-law functions of
+//                      util/UserRateLaws.c as device functions)
+//   kpp_fun            ODE right-hand side, aggregate form (src/gen.c:642-724)
+//   kpp_jac_sp         sparse Jacobian in the LU pattern (src/gen.c:1185-1322)
+//   kpp_decomp         fully unrolled no-pivot sparse LU; same operation
+//                      sequence as the loop of util/sutil.c:2-23
+//   kpp_solve          unrolled forward/backward substitution
+//                      (src/gen.c:1960-2034)
+//
+// Arithmetic is the reference's, operation for operation: expression trees
+// are built with the same constant folding (multiplying by a constant 1
+// drops the constant, a constant 0 annihilates, adding 0 drops the term,
+// src/code.c:519-590), constants are the single-precision values KPP stores,
+// written with "%g" (src/code.c:474-476, src/code_c.c:66), sums run left to
+// right over equations in order, and the printed expressions are
+// parenthesised so that C evaluates exactly the tree.  Built without FMA
+// contraction the device code then rounds like the reference's C code; only
+// the libm-class functions (exp, pow, log10, cos) can differ by an ulp.
+#include <algorithm>
+#include <cctype>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <sstream>
+
+#include "mechanism.hpp"
+
+namespace kppcu {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Expression trees
+// ---------------------------------------------------------------------------
+enum NodeKind { N_CONST, N_LEAF, N_ADD, N_SUB, N_MUL, N_DIV };
+
+struct Node;
+using P = std::shared_ptr<Node>;
+
+struct Node {
+  NodeKind kind;
+  int sign = 1;      // leaves and constants carry a sign
+  float value = 0;   // |constant|, single precision
+  std::string text;  // leaf text
+  P l, r;
+};
+
+P cnst(double v) {
+  P n = std::make_shared<Node>();
+  n->kind = N_CONST;
+  float f = (float)v;
+  if (f < 0) { f = -f; n->sign = -1; }
+  n->value = f;
+  return n;
+}
+P leaf(const std::string& t) {
+  P n = std::make_shared<Node>();
+  n->kind = N_LEAF;
+  n->text = t;
+  return n;
+}
+P bin(NodeKind k, P a, P b) {
+  P n = std::make_shared<Node>();
+  n->kind = k;
+  n->l = std::move(a);
+  n->r = std::move(b);
+  return n;
+}
+bool is_const(const P& n, float v) { return n && n->kind == N_CONST && n->value == v; }
+
+P add(P a, P b) {
+  if (!a) return b;
+  if (!b) return a;
+  if (is_const(a, 0)) return b;
+  if (is_const(b, 0)) return a;
+  return bin(N_ADD, a, b);
+}
+P sub(P a, P b) {
+  if (!a) return bin(N_SUB, nullptr, b);
+  if (!b) return a;
+  if (is_const(a, 0)) return bin(N_SUB, nullptr, b);
+  if (is_const(b, 0)) return a;
+  return bin(N_SUB, a, b);
+}
+P mul(P a, P b) {
+  if (!a) return b;
+  if (!b) return a;
+  if (is_const(a, 1)) { b->sign *= a->sign; return b; }
+  if (is_const(b, 1)) return a;  // the sign of b is not applied (src/code.c:555-559)
+  if (is_const(a, 0)) return a;
+  if (is_const(b, 0)) return b;
+  return bin(N_MUL, a, b);
+}
+P divide(P a, P b) {
+  if (!a) return bin(N_DIV, cnst(1), b);
+  if (!b) return a;
+  if (is_const(b, 1)) return a;
+  return bin(N_DIV, a, b);
+}
+
+std::string fmt_g(float v) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%g", (double)v);
+  std::string s = buf;
+  // make it a double literal without changing its value
+  if (s.find_first_of(".eEn") == std::string::npos) s += ".0";
+  return s;
+}
+
+int prec(const P& n) {
+  switch (n->kind) {
+    case N_ADD: case N_SUB: return 1;
+    case N_MUL: case N_DIV: return 2;
+    default: return 3;
+  }
+}
+
+// C text that evaluates exactly the tree: left-associative chains print
+// without parentheses, anything else is parenthesised.
+std::string print(const P& n, int parent, bool right) {
+  std::string s;
+  switch (n->kind) {
+    case N_CONST: s = fmt_g(n->value); return n->sign < 0 ? "(-" + s + ")" : s;
+    case N_LEAF: return n->sign < 0 ? "(-" + n->text + ")" : n->text;
+    case N_ADD: s = print(n->l, 1, false) + " + " + print(n->r, 1, true); break;
+    case N_SUB:
+      s = n->l ? print(n->l, 1, false) + " - " + print(n->r, 1, true) : "-" + print(n->r, 3, true);
+      break;
+    case N_MUL: s = print(n->l, 2, false) + "*" + print(n->r, 2, true); break;
+    case N_DIV: s = print(n->l, 2, false) + "/" + print(n->r, 2, true); break;
+  }
+  int p = prec(n);
+  if (p < parent || (right && p == parent)) return "(" + s + ")";
+  return s;
+}
+std::string print(const P& n) { return print(n, 0, false); }
+
+// FP64 add/sub/mul/div operations the tree evaluates (unary minus is free).
+long count_ops(const P& n) {
+  if (!n) return 0;
+  switch (n->kind) {
+    case N_ADD: case N_MUL: case N_DIV: return 1 + count_ops(n->l) + count_ops(n->r);
+    case N_SUB: return (n->l ? 1 : 0) + count_ops(n->l) + count_ops(n->r);
+    default: return 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mechanism accessors in the final species order
+// ---------------------------------------------------------------------------
+struct View {
+  const Mechanism& m;
+  explicit View(const Mechanism& mm) : m(mm) {}
+  float left(int spc, int eq) const { return m.left[m.spc_slot[spc]][eq]; }
+  float net(int spc, int eq) const { return m.net[m.spc_slot[spc]][eq]; }
+  std::string name(int spc) const { return m.table[m.order[m.spc_slot[spc]]].name; }
+  // rate factor: RCT[j] for expressions, the float constant for numbers
+  P rconst(int eq) const {
+    const Reaction& r = m.reactions[eq];
+    if (r.kind == RATE_NUMBER) return cnst(r.number);
+    return leaf("RCT[" + std::to_string(eq) + "]");
+  }
+  // product of the reactant concentrations of equation eq, leaving out one
+  // occurrence of variable species `skip` (-1: none)
+  P reactants(P prod, int eq, int skip) const {
+    for (int i = 0; i < m.nvar; i++) {
+      int k = (int)left(i, eq) - (i == skip ? 1 : 0);
+      for (int c = 0; c < k; c++) prod = mul(prod, leaf("V[" + std::to_string(i) + "]"));
+    }
+    for (int i = m.nvar; i < m.nspec; i++) {
+      int k = (int)left(i, eq);
+      for (int c = 0; c < k; c++) prod = mul(prod, leaf("F[" + std::to_string(i - m.nvar) + "]"));
+    }
+    return prod;
+  }
+};
+
+std::string c_string(const std::string& s) {
+  std::string o = "\"";
+  for (char c : s) {
+    if (c == '"' || c == '\\') o += '\\';
+    o += c;
+  }
+  return o + "\"";
+}
+
+void emit_int_table(std::ostream& o, const char* name, const std::vector<int>& v) {
+  o << "static const int " << name << "[" << (v.empty() ? 1 : v.size()) << "] = {";
+  for (size_t i = 0; i < v.size(); i++) o << (i % 16 == 0 ? "\n    " : " ") << v[i] << ",";
+  if (v.empty()) o << "0";
+  o << "};\n";
+}
+
+enum RateClass { RC_STATIC = 0, RC_SUN = 1, RC_DYNAMIC = 2 };
+
+// What a rate expression depends on: only TEMP/CFACTOR and pure functions
+// (static for a cell), also SUN, or anything else (time, concentrations,
+// user variables: recomputed at every evaluation).
+int classify_rate(const std::string& e) {
+  static const char* pure[] = {"ARR_abc", "ARR_ab", "ARR_ac", "EP2", "EP3", "FALL", "exp",
+                               "pow", "log", "log10", "sqrt", "cos", "sin", "tan", "fabs",
+                               "fmin", "fmax", "TEMP", "CFACTOR", "double", "float"};
+  int cls = RC_STATIC;
+  size_t i = 0;
+  while (i < e.size()) {
+    char c = e[i];
+    if (std::isdigit((unsigned char)c) || (c == '.' && i + 1 < e.size() && std::isdigit((unsigned char)e[i + 1]))) {
+      while (i < e.size() && (std::isdigit((unsigned char)e[i]) || e[i] == '.')) i++;
+      if (i < e.size() && std::strchr("eEdD", e[i])) {
+        size_t k = i + 1;
+        if (k < e.size() && (e[k] == '+' || e[k] == '-')) k++;
+        if (k < e.size() && std::isdigit((unsigned char)e[k])) {
+          i = k;
+          while (i < e.size() && std::isdigit((unsigned char)e[i])) i++;
+        }
+      }
+      continue;
+    }
+    if (std::isalpha((unsigned char)c) || c == '_') {
+      size_t b = i;
+      while (i < e.size() && (std::isalnum((unsigned char)e[i]) || e[i] == '_')) i++;
+      std::string id = e.substr(b, i - b);
+      bool known = false;
+      for (const char* p : pure)
+        if (id == p) known = true;
+      if (known) continue;
+      if (id == "SUN") cls = std::max(cls, (int)RC_SUN);
+      else cls = RC_DYNAMIC;
+      continue;
+    }
+    i++;
+  }
+  return cls;
+}
+
+}  // namespace
+
+bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
+  View vw(m);
+  long ops_fun = 0, ops_jac = 0, ops_decomp = 0, ops_solve = 0;
+  const int nvar = m.nvar, nfix = m.nfix, nspec = m.nspec, nr = m.nreact();
+  std::ostringstream o;
+
+  o << "// Generated by kppcu, the KPP mechanism compiler of kpp_b200.  Do not edit.\n"
+    << "// Mechanism: " << m.root << "\n"
+    << "#pragma once\n\n"
+    << "#define KPP_MECH_NAME " << c_string(m.root) << "\n"
+    << "#define KPP_NVAR " << nvar << "\n"
+    << "#define KPP_NFIX " << (nfix > 0 ? nfix : 1) << "\n"
+    << "#define KPP_NFIX_TRUE " << nfix << "\n"
+    << "#define KPP_NSPEC " << nspec << "\n"
+    << "#define KPP_NVARACT " << m.nvaract << "\n"
+    << "#define KPP_NREACT " << nr << "\n"
+    << "#define KPP_NONZERO " << m.nonzero << "\n"
+    << "#define KPP_LU_NONZERO " << m.lu_nonzero << "\n"
+    << "#define KPP_CFACTOR " << std::to_string(m.cfactor) << "\n\n";
+  {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.17g", m.cfactor);
+    o << "#undef KPP_CFACTOR\n#define KPP_CFACTOR " << buf << "\n\n";
+  }
+  o << "// Species indices (variable species first, then fixed species).\n";
+  for (int i = 0; i < nspec; i++) o << "#define ind_" << vw.name(i) << " " << i << "\n";
+  for (int i = nvar; i < nspec; i++) o << "#define indf_" << vw.name(i) << " " << (i - nvar) << "\n";
+  o << "\n";
+
+  // ---- host/device tables
+  o << "namespace kpp_mech {\n\n";
+  o << "static const char* const kSpeciesNames[" << nspec << "] = {";
+  for (int i = 0; i < nspec; i++) o << (i % 6 == 0 ? "\n    " : " ") << c_string(vw.name(i)) << ",";
+  o << "};\n\n";
+  o << "// #INITVALUES, before the CFACTOR scaling (values in mechanism units)\n";
+  o << "static const double kInitialValues[" << nspec << "] = {";
+  for (int i = 0; i < nspec; i++) {
+    const Species& s = m.table[m.order[m.spc_slot[i]]];
+    std::string v = !s.ival.empty() ? s.ival : (i < nvar ? m.var_default : m.fix_default);
+    for (char& ch : v)
+      if (ch == 'd' || ch == 'D') ch = 'e';
+    o << (i % 6 == 0 ? "\n    " : " ") << "(" << v << "),";
+  }
+  o << "};\n\n";
+  emit_int_table(o, "kLuIRow", m.lu_irow);
+  emit_int_table(o, "kLuICol", m.lu_icol);
+  emit_int_table(o, "kLuCRow", m.lu_crow);
+  emit_int_table(o, "kLuDiag", m.lu_diag);
+  o << "\n";
+  std::vector<int> kinds;
+  for (const Reaction& r : m.reactions) kinds.push_back((int)r.kind);
+  emit_int_table(o, "kRateKind", kinds);
+  o << "\n}  // namespace kpp_mech\n\n";
+
+  // ---- user device code from the CUDA_* inline blocks
+  for (const char* ctx : {"CUDA_GLOBAL", "CUDA_UTIL", "CUDA_RATES"}) {
+    auto it = m.inline_code.find(ctx);
+    if (it != m.inline_code.end()) o << "// #INLINE " << ctx << "\n" << it->second << "\n";
+  }
+
+  // ---- rate constants, split by what they depend on
+  // Every rate is recomputed from the same inputs wherever the reference
+  // recomputes it, so hoisting a rate out of the time loop when its inputs
+  // are constant for the cell gives the same bits.
+  std::vector<int> rclass(nr, RC_STATIC);
+  bool rconst_inline = m.inline_code.count("CUDA_RCONST") > 0;
+  for (int j = 0; j < nr; j++) {
+    const Reaction& r = m.reactions[j];
+    if (r.kind == RATE_NUMBER) { rclass[j] = -1; continue; }
+    rclass[j] = rconst_inline ? RC_DYNAMIC : classify_rate(r.rate);
+  }
+  const char* kRateMacros =
+      "#define ARR_abc(a0, b0, c0) kpp_arr_abc(TEMP, (float)(a0), (float)(b0), (float)(c0))\n"
+      "#define ARR_ab(a0, b0) kpp_arr_ab(TEMP, (float)(a0), (float)(b0))\n"
+      "#define ARR_ac(a0, c0) kpp_arr_ac(TEMP, (float)(a0), (float)(c0))\n"
+      "#define EP2(a0, c0, a2, c2, a3, c3) kpp_ep2(TEMP, CFACTOR, (float)(a0), (float)(c0), "
+      "(float)(a2), (float)(c2), (float)(a3), (float)(c3))\n"
+      "#define EP3(a1, c1, a2, c2) kpp_ep3(TEMP, CFACTOR, (float)(a1), (float)(c1), (float)(a2), "
+      "(float)(c2))\n"
+      "#define FALL(a0, b0, c0, a1, b1, c1, cf) kpp_fall(TEMP, CFACTOR, (float)(a0), (float)(b0), "
+      "(float)(c0), (float)(a1), (float)(b1), (float)(c1), (float)(cf))\n";
+  const char* kRateUndef = "#undef ARR_abc\n#undef ARR_ab\n#undef ARR_ac\n#undef EP2\n#undef EP3\n#undef FALL\n";
+  int ncls[3] = {0, 0, 0};
+  for (int j = 0; j < nr; j++)
+    if (rclass[j] >= 0) ncls[rclass[j]]++;
+  o << "// Rate constants by dependence: " << ncls[RC_STATIC] << " depend only on TEMP and CFACTOR,\n"
+    << "// " << ncls[RC_SUN] << " also on SUN, " << ncls[RC_DYNAMIC]
+    << " on the time or the concentrations.\n"
+    << "#define KPP_RATES_SUN " << ncls[RC_SUN] << "\n"
+    << "#define KPP_RATES_DYNAMIC " << ncls[RC_DYNAMIC] << "\n\n";
+  const char* names[3] = {"kpp_rconst_static", "kpp_rconst_sun", "kpp_rconst_dynamic"};
+  for (int c = 0; c < 3; c++) {
+    o << "template <class TR, class TV, class TF>\n"
+      << "__device__ __forceinline__ void " << names[c]
+      << "(TR& RCONST, const double TIME, const double TEMP, const double CFACTOR,\n"
+         "    double SUN, const TV& VAR, const TF& FIX) {\n"
+         "  (void)TIME; (void)TEMP; (void)CFACTOR; (void)SUN; (void)VAR; (void)FIX;\n"
+      << kRateMacros;
+    if (c == RC_DYNAMIC && rconst_inline)
+      o << "  // #INLINE CUDA_RCONST\n" << m.inline_code.at("CUDA_RCONST") << "\n";
+    for (int j = 0; j < nr; j++) {
+      if (rclass[j] == c) o << "  RCONST[" << j << "] = (" << m.reactions[j].rate << ");\n";
+      // constant rates are folded into Fun/Jac_SP; the reference's
+      // Initialize() also stores them in RCONST (as single-precision values)
+      if (c == RC_STATIC && rclass[j] < 0)
+        o << "  RCONST[" << j << "] = " << fmt_g(m.reactions[j].number) << ";\n";
+    }
+    o << kRateUndef << "}\n\n";
+  }
+  o << "// All rate constants at time TIME (Update_RCONST, src/gen.c:2343-2473).\n"
+       "template <class TR, class TV, class TF>\n"
+       "__device__ __forceinline__ void kpp_update_rconst(TR& RCONST, const double TIME,\n"
+       "    const double TEMP, const double CFACTOR, double SUN, const TV& VAR, const TF& FIX) {\n"
+       "  kpp_rconst_static(RCONST, TIME, TEMP, CFACTOR, SUN, VAR, FIX);\n"
+       "  kpp_rconst_sun(RCONST, TIME, TEMP, CFACTOR, SUN, VAR, FIX);\n"
+       "  kpp_rconst_dynamic(RCONST, TIME, TEMP, CFACTOR, SUN, VAR, FIX);\n"
+       "}\n\n";
+
+  // ---- Fun (aggregate form)
+  o << "// ODE right-hand side Vdot = f(V) of one cell; A holds the equation rates.\n"
+       "template <class TV, class TF, class TR, class TO, class TA>\n"
+       "__device__ __forceinline__ void kpp_fun(const TV& V, const TF& F, const TR& RCT,\n"
+       "    TO& Vdot, TA& A) {\n"
+       "  (void)F; (void)RCT;\n";
+  for (int j = 0; j < nr; j++) {
+    bool used = false;
+    for (int i = 0; i < nvar; i++)
+      if (vw.net(i, j) != 0) { used = true; break; }
+    if (!used) continue;
+    P prod = vw.reactants(vw.rconst(j), j, -1);
+    ops_fun += count_ops(prod);
+    o << "  A[" << j << "] = " << print(prod) << ";\n";
+  }
+  for (int i = 0; i < nvar; i++) {
+    P sum = cnst(0);
+    for (int j = 0; j < nr; j++) sum = add(sum, mul(cnst(vw.net(i, j)), leaf("A[" + std::to_string(j) + "]")));
+    ops_fun += count_ops(sum);
+    o << "  Vdot[" << i << "] = " << print(sum) << ";\n";
+  }
+  o << "}\n\n";
+
+  // ---- Jac_SP
+  std::vector<std::vector<int>> bidx(nr, std::vector<int>(nvar, -1));
+  int nb = 0;
+  for (int i = 0; i < nr; i++)
+    for (int j = 0; j < nvar; j++)
+      if (vw.left(j, i) != 0) bidx[i][j] = nb++;
+  o << "#define KPP_NJAC_TMP " << (nb > 0 ? nb : 1) << "\n\n";
+  o << "// Sparse Jacobian of one cell in the LU pattern (fill-in entries are 0);\n"
+       "// NEG = true writes its negation (the -Jac0 of ros_PrepareMatrix).  B holds\n"
+       "// the partial derivatives of the equation rates (KPP_NJAC_TMP entries).\n"
+       "template <bool NEG, class TV, class TF, class TR, class TJ, class TB>\n"
+       "__device__ __forceinline__ void kpp_jac_sp(const TV& V, const TF& F, const TR& RCT,\n"
+       "    TJ& JVS, TB& B) {\n"
+       "  (void)V; (void)F; (void)RCT;\n";
+  for (int i = 0; i < nr; i++)
+    for (int j = 0; j < nvar; j++) {
+      if (bidx[i][j] < 0) continue;
+      P prod = mul(vw.rconst(i), cnst(vw.left(j, i)));
+      prod = vw.reactants(prod, i, j);
+      ops_jac += count_ops(prod);
+      o << "  B[" << bidx[i][j] << "] = " << print(prod) << ";\n";
+    }
+  {
+    int n = 0;
+    for (int i = 0; i < nvar; i++)
+      for (int j = 0; j < nvar; j++) {
+        if (m.lustruct[i][j]) {
+          P sum = cnst(0);
+          for (int k = 0; k < nr; k++)
+            if (vw.net(i, k) * (bidx[k][j] >= 0 ? 1.0f : 0.0f) != 0)
+              sum = add(sum, mul(cnst(vw.net(i, k)), leaf("B[" + std::to_string(bidx[k][j]) + "]")));
+          ops_jac += count_ops(sum);
+          o << "  JVS[" << n << "] = NEG ? -(" << print(sum) << ") : (" << print(sum) << ");\n";
+          n++;
+        } else if (i == j) {
+          o << "  JVS[" << n << "] = NEG ? -0.0 : 0.0;\n";
+          n++;
+        }
+      }
+  }
+  o << "}\n\n";
+
+  // ---- diagonal shift of ros_PrepareMatrix (int/rosenbrock.c:720-723)
+  o << "// JVS[diag] += v for every row (the 1/(h*gamma) shift of the Rosenbrock matrix).\n"
+       "template <class TJ>\n"
+       "__device__ __forceinline__ void kpp_add_diagonal(TJ& JVS, const double v) {\n";
+  for (int i = 0; i < nvar; i++)
+    o << "  JVS[" << m.lu_diag[i] << "] = JVS[" << m.lu_diag[i] << "] + v;\n";
+  o << "}\n\n";
+
+  // ---- KppDecomp, unrolled
+  {
+    std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
+    for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
+    o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
+         "// entry of row k is zero on entry to its elimination, 0 on success.\n"
+         "template <class TJ>\n"
+         "__device__ __forceinline__ int kpp_decomp(TJ& JVS) {\n"
+         "  double a;\n";
+    for (int k = 0; k < nvar; k++) {
+      o << "  if (JVS[" << m.lu_diag[k] << "] == 0.0) return " << (k + 1) << ";\n";
+      for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+        int j = m.lu_icol[kk];
+        ops_decomp += 1;
+        o << "  a = -JVS[" << kk << "] / JVS[" << m.lu_diag[j] << "];\n";
+        o << "  JVS[" << kk << "] = -a;\n";
+        for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
+          int t = pos[k][m.lu_icol[jj]];
+          ops_decomp += 2;
+          o << "  JVS[" << t << "] = JVS[" << t << "] + a*JVS[" << jj << "];\n";
+        }
+      }
+    }
+    o << "  return 0;\n}\n\n";
+  }
+
+  // ---- KppSolve, unrolled
+  o << "// Solve (LU) x = b in place, b given in X.\n"
+       "template <class TJ, class TX>\n"
+       "__device__ __forceinline__ void kpp_solve(const TJ& JVS, TX& X) {\n";
+  for (int i = 0; i < nvar; i++) {
+    int b = m.lu_crow[i], e = m.lu_diag[i];
+    if (b < e) {
+      P sum = leaf("X[" + std::to_string(i) + "]");
+      for (int j = b; j < e; j++)
+        sum = sub(sum, mul(leaf("JVS[" + std::to_string(j) + "]"),
+                           leaf("X[" + std::to_string(m.lu_icol[j]) + "]")));
+      ops_solve += count_ops(sum);
+      o << "  X[" << i << "] = " << print(sum) << ";\n";
+    }
+  }
+  for (int i = nvar - 1; i >= 0; i--) {
+    P sum = leaf("X[" + std::to_string(i) + "]");
+    for (int j = m.lu_diag[i] + 1; j < m.lu_crow[i + 1]; j++)
+      sum = sub(sum, mul(leaf("JVS[" + std::to_string(j) + "]"),
+                         leaf("X[" + std::to_string(m.lu_icol[j]) + "]")));
+    sum = divide(sum, leaf("JVS[" + std::to_string(m.lu_diag[i]) + "]"));
+    ops_solve += count_ops(sum);
+    o << "  X[" << i << "] = " << print(sum) << ";\n";
+  }
+  o << "}\n\n";
+  o << "// FP64 add/sub/mul/div operations per call of each function (for the\n"
+       "// FP64 roofline; rate constants and the integrator's vector operations\n"
+       "// are counted separately).\n"
+    << "#define KPP_OPS_FUN " << ops_fun << "\n"
+    << "#define KPP_OPS_JAC " << ops_jac << "\n"
+    << "#define KPP_OPS_DECOMP " << ops_decomp << "\n"
+    << "#define KPP_OPS_SOLVE " << ops_solve << "\n";
+
+  std::ofstream f(out_prefix + ".cuh");
+  if (!f) return false;
+  f << o.str();
+  return (bool)f;
+}
+
+}  // namespace kppcu

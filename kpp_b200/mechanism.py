@@ -1,0 +1,213 @@
+"""Python host layer over the C ABI of include/kpp_b200.h.
+
+A `Mechanism` wraps one mechanism library (libkpp_b200_<mech>.so) through
+ctypes.  Device arrays are torch CUDA tensors of float64/int32 in the ABI's
+layout: [rows, ld] with the cell index fastest (row-major, contiguous), so the
+pointer of tensor[i, c] is var + i*ld + c exactly as the ABI expects.
+
+`Mechanism.integrate` is the batched counterpart of the generated C
+`INTEGRATE(TIN, TOUT)` (int/rosenbrock.c:94-133): it calls the batched
+Rosenbrock for every cell with the caller's controls and returns the warm
+start (Hexit) for the next call, as INTEGRATE keeps STEPMIN = RPAR[11].
+
+There is no CPU fallback: constructing a Mechanism fails when its library is
+missing, and the integration entry points require CUDA tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Optional, Sequence
+
+import torch
+
+from . import controls as _controls
+
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+KPP_B200_OK = 0
+
+
+class KppError(RuntimeError):
+    pass
+
+
+@dataclass
+class RosenbrockResult:
+    """Per-cell outputs: IERR, ISTATUS (IPAR[10..17]) and RSTATUS (Texit, Hexit)."""
+    ierr: torch.Tensor      # [ncells] int32
+    istatus: torch.Tensor   # [8, ncells] int32: Nfun Njac Nstp Nacc Nrej Ndec Nsol Nsng
+    rstatus: torch.Tensor   # [2, ncells] float64: Texit, Hexit
+
+    @property
+    def hexit(self) -> torch.Tensor:
+        return self.rstatus[1]
+
+
+def library_path(name: str) -> Path:
+    return LIB_DIR / f"libkpp_b200_{name}.so"
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return None if t is None else _vp(t.data_ptr())
+
+
+class Mechanism:
+    """One compiled mechanism: its sizes, species, sparsity and entry points."""
+
+    def __init__(self, name: str, path: Optional[Path] = None):
+        path = Path(path) if path else library_path(name)
+        if not path.exists():
+            raise KppError(f"kpp_b200 library for mechanism {name!r} not found at {path}; "
+                           f"build it with `python -m kpp_b200.build {name}`")
+        self.path = path
+        self.lib = ctypes.CDLL(str(path))
+        self._declare()
+        dims = (ctypes.c_int * 6)()
+        self._check(self.lib.kpp_b200_dims(dims))
+        self.nvar, self.nfix, self.nspec, self.nreact, self.lu_nonzero, self.nonzero = list(dims)
+        self.name = self.lib.kpp_b200_mechanism_name().decode()
+        self.species = [self.lib.kpp_b200_species_name(i).decode() for i in range(self.nspec)]
+
+    # -- ctypes prototypes -------------------------------------------------
+    def _declare(self):
+        L = self.lib
+        L.kpp_b200_dims.argtypes = [_c_int_p]
+        L.kpp_b200_mechanism_name.restype = ctypes.c_char_p
+        L.kpp_b200_species_name.argtypes = [ctypes.c_int]
+        L.kpp_b200_species_name.restype = ctypes.c_char_p
+        L.kpp_b200_initial_values.argtypes = [_c_double_p, _c_double_p]
+        L.kpp_b200_lu_pattern.argtypes = [_c_int_p] * 4
+        L.kpp_b200_last_error.restype = ctypes.c_char_p
+        L.kpp_b200_workspace_bytes.argtypes = [ctypes.c_int]
+        L.kpp_b200_workspace_bytes.restype = ctypes.c_size_t
+        ros = [ctypes.c_int, ctypes.c_int] + [_vp] * 9 + [_c_int_p, _c_double_p, _vp, _vp, _vp, _vp]
+        L.kpp_b200_rosenbrock.argtypes = ros + [_vp]
+        L.kpp_b200_rosenbrock_ws.argtypes = ros + [_vp, ctypes.c_size_t, _vp]
+        L.kpp_b200_fun_jac.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 4
+        L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
+
+    def _check(self, rc: int):
+        if rc != KPP_B200_OK:
+            raise KppError(f"kpp_b200 error {rc}: {self.lib.kpp_b200_last_error().decode()}")
+
+    # -- mechanism description --------------------------------------------
+    def initial_values(self):
+        """(C[NSPEC] after Initialize(), CFACTOR)."""
+        c = (ctypes.c_double * self.nspec)()
+        cf = ctypes.c_double()
+        self._check(self.lib.kpp_b200_initial_values(c, ctypes.byref(cf)))
+        return list(c), cf.value
+
+    def lu_pattern(self):
+        n, nz = self.nvar, self.lu_nonzero
+        irow, icol = (ctypes.c_int * nz)(), (ctypes.c_int * nz)()
+        crow, diag = (ctypes.c_int * (n + 1))(), (ctypes.c_int * (n + 1))()
+        self._check(self.lib.kpp_b200_lu_pattern(irow, icol, crow, diag))
+        return list(irow), list(icol), list(crow), list(diag)
+
+    def index(self, species: str) -> int:
+        return self.species.index(species)
+
+    def workspace_bytes(self, ncells: int) -> int:
+        return int(self.lib.kpp_b200_workspace_bytes(ncells))
+
+    # -- batched entry points ---------------------------------------------
+    @staticmethod
+    def _dev(t, dtype, name):
+        if t is None:
+            return None
+        if not (isinstance(t, torch.Tensor) and t.is_cuda):
+            raise KppError(f"{name} must be a CUDA tensor (the path has no CPU fallback)")
+        if t.dtype != dtype or not t.is_contiguous():
+            raise KppError(f"{name} must be a contiguous {dtype} tensor")
+        return t
+
+    def rosenbrock(self, var: torch.Tensor, fix: torch.Tensor, temp: torch.Tensor,
+                   tstart: torch.Tensor, tend: torch.Tensor, atol: torch.Tensor,
+                   rtol: torch.Tensor, ipar: Sequence[int], rpar: Sequence[float],
+                   cfactor: Optional[torch.Tensor] = None, sun: Optional[torch.Tensor] = None,
+                   hstart: Optional[torch.Tensor] = None, ncells: Optional[int] = None,
+                   out: Optional[RosenbrockResult] = None,
+                   workspace: Optional[torch.Tensor] = None,
+                   stream: Optional[torch.cuda.Stream] = None) -> RosenbrockResult:
+        """Batched Rosenbrock (kpp_b200_rosenbrock).  var [NVAR, ld] is updated
+        in place; returns IERR/ISTATUS/RSTATUS.  Asynchronous on `stream`."""
+        f64, i32 = torch.float64, torch.int32
+        self._dev(var, f64, "var")
+        ld = var.shape[1]
+        n = ld if ncells is None else ncells
+        for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                      (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun"),
+                      (hstart, "hstart")):
+            self._dev(t, f64, nm)
+        if out is None:
+            out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
+                                   istatus=torch.empty(8, ld, dtype=i32, device=var.device),
+                                   rstatus=torch.empty(2, ld, dtype=f64, device=var.device))
+        ip = (ctypes.c_int * 20)(*[int(x) for x in ipar])
+        rp = (ctypes.c_double * 20)(*[float(x) for x in rpar])
+        s = stream if stream is not None else torch.cuda.current_stream(var.device)
+        args = [n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun),
+                _ptr(tstart), _ptr(tend), _ptr(atol), _ptr(rtol), ip, rp, _ptr(hstart),
+                _ptr(out.istatus), _ptr(out.rstatus), _ptr(out.ierr)]
+        if workspace is not None:
+            self._check(self.lib.kpp_b200_rosenbrock_ws(
+                *args, _ptr(workspace), workspace.numel() * workspace.element_size(),
+                _vp(s.cuda_stream)))
+        else:
+            self._check(self.lib.kpp_b200_rosenbrock(*args, _vp(s.cuda_stream)))
+        return out
+
+    def fun_jac(self, var, fix, temp, time: float, cfactor=None, sun=None,
+                want=("rconst", "vdot", "jvs"), stream=None):
+        """Batched Update_RCONST / Fun / Jac_SP at one time (kpp_b200_fun_jac)."""
+        f64 = torch.float64
+        self._dev(var, f64, "var")
+        ld = var.shape[1]
+        dev = var.device
+        rconst = torch.empty(self.nreact, ld, dtype=f64, device=dev) if "rconst" in want else None
+        vdot = torch.empty(self.nvar, ld, dtype=f64, device=dev) if "vdot" in want else None
+        jvs = torch.empty(self.lu_nonzero, ld, dtype=f64, device=dev) if "jvs" in want else None
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        self._check(self.lib.kpp_b200_fun_jac(ld, ld, _ptr(var), _ptr(fix), _ptr(temp),
+                                              _ptr(cfactor), _ptr(sun), float(time),
+                                              _ptr(rconst), _ptr(vdot), _ptr(jvs),
+                                              _vp(s.cuda_stream)))
+        return rconst, vdot, jvs
+
+    def decomp_solve(self, jvs: torch.Tensor, x: Optional[torch.Tensor] = None, stream=None):
+        """In-place batched KppDecomp (+ KppSolve of x); returns ising [ld]."""
+        self._dev(jvs, torch.float64, "jvs")
+        ld = jvs.shape[1]
+        ising = torch.empty(ld, dtype=torch.int32, device=jvs.device)
+        s = stream if stream is not None else torch.cuda.current_stream(jvs.device)
+        self._check(self.lib.kpp_b200_decomp_solve(ld, ld, _ptr(jvs), _ptr(x), _ptr(ising),
+                                                   _vp(s.cuda_stream)))
+        return ising
+
+    # -- INTEGRATE-style driver -------------------------------------------
+    def integrate(self, var, fix, temp, tin, tout, atol, rtol, method: str = "rodas3",
+                  stepmin=None, cfactor=None, sun=None, **controls) -> RosenbrockResult:
+        """One chemistry step for every cell, like the generated INTEGRATE(TIN,
+        TOUT): non-autonomous, the given method, starting step `stepmin`
+        (per cell, the previous call's Hexit; None = default)."""
+        ipar, rpar = _controls.make_controls(method=method, scalar_tol=atol.numel() == 1,
+                                             **controls)
+        return self.rosenbrock(var, fix, temp, tin, tout, atol, rtol, ipar, rpar,
+                               cfactor=cfactor, sun=sun, hstart=stepmin)
+
+
+_loaded = {}
+
+
+def load(name: str) -> Mechanism:
+    """Load (once per process) the library of mechanism `name`."""
+    if name not in _loaded:
+        _loaded[name] = Mechanism(name)
+    return _loaded[name]

@@ -10,7 +10,8 @@
 #   oracle/_ref/kpp                               reference generator
 #   oracle/_ref/<mech>/<mech>_*.c|h               reference-generated model
 #   oracle/_ref/<mech>/libkppref_<mech>.so        -O (reference flags, util/Makefile_c:3)
-#   oracle/_ref/<mech>/libkppref_<mech>_O3.so     -O3 -march=native (timing only)
+#   oracle/_ref/<mech>/libkppref_<mech>_O3.so     -O3 -march=x86-64-v3 (FMA contraction:
+#                                                 the same code with another valid rounding)
 #
 # The generator is compiled from the unchanged sources in $KPP_REF/src; only
 # the flex/bison front end is replaced by oracle/refkpp/frontend.c because
@@ -62,9 +63,12 @@ for mech in "${MECHS[@]}"; do
 #MEX        OFF
 #INLINE C_GLOBAL
   extern double kppref_sun_override;
+  extern int kppref_sun_ulps;
 #ENDINLINE
 #INLINE C_RCONST
   if (kppref_sun_override >= 0.0) SUN = kppref_sun_override;
+  if (kppref_sun_ulps > 0) SUN = nextafter(SUN, 2.0);
+  if (kppref_sun_ulps < 0) SUN = nextafter(SUN, -1.0);
 #ENDINLINE
 EOF
   (cd "$d" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
@@ -76,7 +80,7 @@ EOF
   inc=(-include "$d/${mech}_Parameters.h" -include "$d/${mech}_Global.h" -include "$d/${mech}_Sparse.h")
   "$CC" -O -Wall -w -fPIC -shared -I"$d" "${srcs[@]}" \
     -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}.so"
-  "$CC" -O3 -march=native -w -fPIC -shared -I"$d" "${srcs[@]}" \
+  "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$d" "${srcs[@]}" \
     -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}_O3.so"
   echo "build_ref: $mech -> $d/libkppref_${mech}.so"
 done

@@ -23,6 +23,10 @@
 ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~*/
 
 double kppref_sun_override = -1.0;
+int kppref_sun_ulps = 0;
+
+/* Test knob: every evaluation moves SUN by one ulp up (1) or down (-1). */
+void kppref_set_sun_ulps(int u) { kppref_sun_ulps = u; }
 
 int Rosenbrock(double Y[], double Tstart, double Tend, double AbsTol[],
                double RelTol[], void (*ode_Fun)(double, double[], double[]),

@@ -1,0 +1,41 @@
+// Host build of kppcu's generated mechanism code (test infrastructure).
+//
+// The generated header is CUDA device code; compiled here as plain C++ for
+// the host (device qualifiers removed, host libm), so tests can compare the
+// emitted arithmetic against the reference's own generated C functions on
+// the CPU, where both use the same libm and compiler: any difference is then
+// an emitter error, not a math-library ulp.
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#include <cmath>
+using std::cos;
+using std::exp;
+using std::log10;
+using std::pow;
+#include "kpp_ratelaws.cuh"
+#include KPP_MECH_HEADER
+
+extern "C" {
+
+void host_rates(double temp, double cfactor, double sun, double t, const double* var,
+                const double* fix, double* rconst) {
+  double s = sun >= 0.0 ? sun : kpp_update_sun(t);
+  kpp_update_rconst(rconst, t, temp, cfactor, s, var, fix);
+}
+
+void host_fun(const double* var, const double* fix, const double* rconst, double* vdot) {
+  double a[KPP_NREACT > 0 ? KPP_NREACT : 1];
+  kpp_fun(var, fix, rconst, vdot, a);
+}
+
+void host_jac(const double* var, const double* fix, const double* rconst, double* jvs) {
+  double b[KPP_NJAC_TMP];
+  kpp_jac_sp<false>(var, fix, rconst, jvs, b);
+}
+
+int host_decomp(double* jvs) { return kpp_decomp(jvs); }
+
+void host_solve(const double* jvs, double* x) { kpp_solve(jvs, x); }
+
+}

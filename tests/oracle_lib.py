@@ -1,0 +1,124 @@
+"""ctypes access to the oracle libraries (test infrastructure only).
+
+oracle/_ref/<mech>/libkppref_<mech>.so holds the reference's own
+KPP-generated C model for <mech> with
+  kppref_integrate  the reference Rosenbrock (int/rosenbrock.c) driven per
+                    cell by oracle/refkpp/batch_driver.c
+  kppor_integrate   the CPU restatement oracle/ros_oracle.c
+  kppref_fun_jac    the generated Update_RCONST / Fun / Jac_SP of one cell
+Both integrate entries take numpy arrays in the ABI layout ([rows, ld],
+cell index fastest).
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parents[1]
+REF_DIR = REPO / "oracle" / "_ref"
+_vp = ctypes.c_void_p
+
+
+def lib_path(mech: str, opt: str = "") -> Path:
+    return REF_DIR / mech / f"libkppref_{mech}{opt}.so"
+
+
+def ensure_built(mechs=("small_strato", "saprc99")) -> bool:
+    """Build the oracle when its libraries are missing and the reference
+    sources are present; True when every library exists afterwards."""
+    if all(lib_path(m).exists() for m in mechs):
+        return True
+    script = REPO / "oracle" / "build_ref.sh"
+    subprocess.run(["bash", str(script), *mechs], check=False,
+                   stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    return all(lib_path(m).exists() for m in mechs)
+
+
+def _p(a):
+    return None if a is None else _vp(a.ctypes.data)
+
+
+class OracleLib:
+    def __init__(self, mech: str, opt: str = ""):
+        self.mech = mech
+        self.lib = ctypes.CDLL(str(lib_path(mech, opt)))
+        d = (ctypes.c_int * 5)()
+        self.lib.kppref_dims(d)
+        self.nvar, self.nfix, self.nspec, self.nreact, self.lu_nonzero = list(d)
+        self.lib.kppref_species_name.restype = ctypes.c_char_p
+        self.species = [self.lib.kppref_species_name(i).decode() for i in range(self.nspec)]
+        for fn in ("kppref_integrate", "kppor_integrate"):
+            getattr(self.lib, fn).argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 15
+        self.lib.kppref_fun_jac.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, _vp, _vp, _vp]
+
+    def initial_values(self):
+        c = np.zeros(self.nspec)
+        cf = ctypes.c_double()
+        self.lib.kppref_initial_values(_p(c), ctypes.byref(cf))
+        return c, cf.value
+
+    def lu_pattern(self):
+        n, nz = self.nvar, self.lu_nonzero
+        irow, icol = np.zeros(nz, np.int32), np.zeros(nz, np.int32)
+        crow, diag = np.zeros(n + 1, np.int32), np.zeros(n + 1, np.int32)
+        self.lib.kppref_lu_pattern(_p(irow), _p(icol), _p(crow), _p(diag))
+        return irow, icol, crow, diag
+
+    def integrate(self, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, cfactor=None,
+                  sun=None, hstart=None, which="ref"):
+        """Integrate every cell; returns (var_out, istatus, rstatus, ierr)."""
+        var = np.ascontiguousarray(var, dtype=np.float64).copy()
+        ld = var.shape[1]
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        fix, temp, tstart, tend = f64(fix), f64(temp), f64(tstart), f64(tend)
+        atol, rtol, cfactor, sun, hstart = f64(atol), f64(rtol), f64(cfactor), f64(sun), f64(hstart)
+        ip = np.ascontiguousarray(ipar, dtype=np.int32)
+        rp = np.ascontiguousarray(rpar, dtype=np.float64)
+        ist = np.zeros((8, ld), np.int32)
+        rst = np.zeros((2, ld), np.float64)
+        ierr = np.zeros(ld, np.int32)
+        fn = self.lib.kppref_integrate if which == "ref" else self.lib.kppor_integrate
+        fn(ld, ld, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun), _p(tstart), _p(tend),
+           _p(atol), _p(rtol), _p(ip), _p(rp), _p(hstart), _p(ist), _p(rst), _p(ierr))
+        return var, ist, rst, ierr
+
+    def set_sun_ulps(self, u: int):
+        """Move SUN by one ulp up (1) / down (-1) at every evaluation (0: off)."""
+        self.lib.kppref_set_sun_ulps(ctypes.c_int(int(u)))
+
+    def fun_jac(self, var, fix, temp, cfactor, sun, t):
+        """Rates, Fun and Jac_SP of one cell (1-D var/fix)."""
+        var = np.ascontiguousarray(var, dtype=np.float64)
+        fix = np.ascontiguousarray(fix, dtype=np.float64)
+        rc = np.zeros(self.nreact)
+        vd = np.zeros(self.nvar)
+        jv = np.zeros(self.lu_nonzero)
+        self.lib.kppref_fun_jac(_p(var), _p(fix), float(temp), float(cfactor),
+                                float(-1.0 if sun is None else sun), float(t), _p(rc), _p(vd), _p(jv))
+        return rc, vd, jv
+
+
+def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, cfactor=None,
+               sun=None, hstart=None):
+    """VAR after the same integration by the reference under other valid
+    last-ulp roundings: compiled with FMA contraction, and with SUN moved by
+    one ulp up and down at every evaluation (the size of a cos() difference
+    in Update_SUN).  Their spread around the reference measures how strongly
+    each entry amplifies last-ulp perturbations."""
+    out = []
+    o3 = OracleLib(mech, "_O3")
+    out.append(o3.integrate(var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, cfactor=cfactor,
+                            sun=sun, hstart=hstart)[0])
+    o = OracleLib(mech)
+    for u in (1, -1):
+        o.set_sun_ulps(u)
+        try:
+            out.append(o.integrate(var, fix, temp, tstart, tend, atol, rtol, ipar, rpar,
+                                   cfactor=cfactor, sun=sun, hstart=hstart)[0])
+        finally:
+            o.set_sun_ulps(0)
+    return np.stack(out)

@@ -1,0 +1,88 @@
+"""The C ABI (CPU): every library loads, exports every entry point that
+include/kpp_b200.h declares, and describes its mechanism like the reference
+(no compute calls: these run without a GPU)."""
+import ctypes
+import json
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from kpp_b200 import Mechanism, from_fortran, library_path, make_controls
+from oracle_lib import REPO
+
+MECHS = ["small_strato", "saprc99"]
+HEADER = REPO / "include" / "kpp_b200.h"
+
+
+def declared_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(kpp_b200_\w+)\s*\(", text)))
+
+
+def exported(lib_path):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib_path)], capture_output=True,
+                         text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+@pytest.mark.parametrize("mech", MECHS)
+def test_library_exports_every_declared_entry(mech):
+    lib = library_path(mech)
+    assert lib.exists(), "build the libraries first: python -m kpp_b200.build"
+    names = declared_functions()
+    assert "kpp_b200_rosenbrock" in names and len(names) >= 8
+    missing = [n for n in names if n not in exported(lib)]
+    assert not missing, missing
+    ctypes.CDLL(str(lib))  # loads without a GPU
+
+
+@pytest.mark.parametrize("mech", MECHS)
+def test_mechanism_description_matches_reference(mech, golden_dir):
+    m = Mechanism(mech)
+    g = json.loads((golden_dir / f"structure_{mech}.json").read_text())
+    assert m.name == mech
+    assert [m.nvar, m.nfix, m.nreact, m.lu_nonzero] == [g["nvar"], g["nfix"], g["nreact"], g["lu_nonzero"]]
+    assert m.species == g["species"]
+    irow, icol, crow, diag = m.lu_pattern()
+    assert icol == g["lu_icol"] and crow == g["lu_crow"] and diag == g["lu_diag"] and irow == g["lu_irow"]
+
+
+@pytest.mark.parametrize("mech", MECHS)
+def test_initial_values_match_reference_initialize(mech):
+    from oracle_lib import OracleLib, ensure_built
+    if not ensure_built():
+        pytest.skip("oracle libraries not built")
+    c, cf = Mechanism(mech).initial_values()
+    rc, rcf = OracleLib(mech).initial_values()
+    assert cf == rcf
+    np.testing.assert_array_equal(np.array(c), rc)
+
+
+def test_entry_points_reject_bad_arguments_without_gpu():
+    m = Mechanism("small_strato")
+    lib = m.lib
+    ip = (ctypes.c_int * 20)()
+    rp = (ctypes.c_double * 20)()
+    # ld < ncells and null pointers fail before touching the device
+    rc = lib.kpp_b200_rosenbrock(4, 2, None, None, None, None, None, None, None, None, None, ip, rp,
+                                 None, None, None, None, None)
+    assert rc == 1 and b"ncells" in lib.kpp_b200_last_error()
+    rc = lib.kpp_b200_rosenbrock(4, 4, None, None, None, None, None, None, None, None, None, ip, rp,
+                                 None, None, None, None, None)
+    assert rc == 1 and b"null" in lib.kpp_b200_last_error()
+    # an empty batch is a no-op
+    assert lib.kpp_b200_rosenbrock(0, 0, None, None, None, None, None, None, None, None, None, ip,
+                                   rp, None, None, None, None, None) == 0
+
+
+def test_controls_layouts():
+    ipar, rpar = make_controls(method="rodas4", scalar_tol=False, max_steps=500, hmin=1e-3,
+                               hmax=100.0, hstart=1.0, facmin=0.1, facmax=5.0, facrej=0.2,
+                               facsafe=0.8, autonomous=True)
+    assert ipar[:4] == [1, 0, 500, 5]
+    assert rpar[:7] == [1e-3, 100.0, 1.0, 0.1, 5.0, 0.2, 0.8]
+    icntrl = [1, 0, 5, 500] + [0] * 16   # ICNTRL(3) = method, ICNTRL(4) = max steps
+    rcntrl = [1e-3, 100.0, 1.0, 0.1, 5.0, 0.2, 0.8] + [0.0] * 13
+    assert from_fortran(icntrl, rcntrl) == (ipar, rpar)

@@ -1,0 +1,184 @@
+"""kppcu, the mechanism compiler (CPU).
+
+  * species order and sparse LU pattern equal the reference generator's, for
+    the benchmark mechanisms (golden structure) and for small mechanisms
+    written here that exercise the language (comments, coefficients, hv,
+    fixed species, #SETFIX, number rates, repeated reactants), by running the
+    reference generator built from its sources next to kppcu;
+  * the emitted device code, compiled for the host, computes the rates, Fun,
+    Jac_SP, LU factorisation and solves bit for bit like the reference's own
+    generated C functions (same compiler, same libm).
+"""
+import ctypes
+import json
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle_lib import OracleLib, REPO, ensure_built
+
+BUILD = REPO / "kpp_b200" / "_build"
+KPP_HOME = os.environ.get("KPP_HOME", "/root/reference")
+HAVE_SOURCES = (Path(KPP_HOME) / "models" / "small_strato.eqn").exists()
+MECHS = ["small_strato", "saprc99"]
+
+
+@pytest.fixture(scope="module")
+def kppcu():
+    from kpp_b200 import build
+    return build.build_kppcu()
+
+
+def run_kppcu(exe, kpp_file, out_prefix, home=KPP_HOME):
+    r = subprocess.run([str(exe), str(kpp_file), "-o", str(out_prefix), "--home", home],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return json.loads(Path(str(out_prefix) + ".json").read_text())
+
+
+@pytest.mark.skipif(not HAVE_SOURCES, reason="mechanism sources not present")
+@pytest.mark.parametrize("mech", MECHS)
+def test_structure_matches_reference_golden(kppcu, mech, tmp_path, golden_dir):
+    got = run_kppcu(kppcu, REPO / "kpp_b200" / "mechanisms" / f"{mech}.kpp", tmp_path / mech)
+    g = json.loads((golden_dir / f"structure_{mech}.json").read_text())
+    assert got["species"] == g["species"]
+    for k in ("nvar", "nfix", "nreact", "lu_nonzero"):
+        assert got[k] == g[k], k
+    for k in ("lu_irow", "lu_icol", "lu_crow", "lu_diag"):
+        assert got[k] == g[k], k
+
+
+# Small mechanisms in the KPP language exercising the front end.
+SMALL = {
+    "toy_chain": """
+#INCLUDE atoms.kpp
+#DEFVAR
+ A = IGNORE; B = IGNORE; C = IGNORE; D = IGNORE;
+#DEFFIX
+ M = IGNORE; { a comment } H2O = IGNORE;
+#EQUATIONS
+<r1> A + hv = 2B        : 1.0e-3*SUN;
+<r2> B + B = C          : 2.5e-11;
+<r3> C + M = A + D      : ARR_ab( 1.0e-12 , -300.0 );
+<r4> D + H2O = 0.5A + 0.5B : (3.0E-15);
+<r5> A + C = B          : 4.0e-12 ;
+""",
+    "toy_setfix": """
+#INCLUDE atoms.kpp
+#DEFVAR
+ X1 = IGNORE; X2 = IGNORE; X3 = IGNORE; X4 = IGNORE; X5 = IGNORE; Y = IGNORE;
+#DEFFIX
+ Z = IGNORE;
+#SETFIX Y;
+#EQUATIONS
+ X1 + X2 = X3            : 1.e-10;
+ X3 + Y = X4 + X1        : 2.0e-12*TEMP;
+ X4 = X5 + X2            : 0.33;
+ X5 + X1 + Z = X2 + X3   : 1.5e-30;
+ X2 + X5 = 2 X1          : 7.7e-13 // trailing comment
+ ;
+ X3 + X4 = X5            : 1.0e-11;
+""",
+}
+
+
+@pytest.mark.skipif(not HAVE_SOURCES, reason="mechanism sources not present")
+@pytest.mark.skipif(not (REPO / "oracle" / "_ref" / "kpp").exists() and not ensure_built(),
+                    reason="reference generator not built")
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_small_mechanisms_match_reference_generator(kppcu, name, tmp_path):
+    eqn = tmp_path / f"{name}.eqn"
+    eqn.write_text(SMALL[name])
+    # kppcu input
+    (tmp_path / f"{name}_cu.kpp").write_text(f"#INCLUDE {name}.eqn\n#LANGUAGE CUDA\n")
+    got = run_kppcu(kppcu, tmp_path / f"{name}_cu.kpp", tmp_path / f"{name}_cu")
+    # reference generator on the same equations, C language
+    (tmp_path / f"{name}.kpp").write_text(
+        f"#INCLUDE {name}.eqn\n#LANGUAGE C\n#INTEGRATOR rosenbrock\n#DRIVER general\n")
+    r = subprocess.run([str(REPO / "oracle" / "_ref" / "kpp"), f"{name}.kpp"], cwd=tmp_path,
+                       env={**os.environ, "KPP_HOME": KPP_HOME}, capture_output=True, text=True)
+    assert r.returncode in (0, 5), r.stdout[-2000:]
+    par = (tmp_path / f"{name}_Parameters.h").read_text()
+    ind = sorted(((int(v), n) for n, v in
+                  (line.split()[1:3] for line in par.splitlines() if line.startswith("#define ind_"))))
+    assert [n[4:] for _, n in ind] == got["species"]
+    sp = (tmp_path / f"{name}_JacobianSP.c").read_text()
+
+    def arr(nm):
+        body = sp.split(nm + "[] = {")[1].split("}")[0]
+        return [int(x) for x in body.replace("\n", " ").split(",") if x.strip()]
+
+    assert arr("LU_ICOL") == got["lu_icol"]
+    assert arr("LU_CROW") == got["lu_crow"]
+    assert arr("LU_DIAG") == got["lu_diag"]
+
+
+# --- emitted arithmetic, compiled for the host -------------------------------
+def _host_lib(mech, tmp_path):
+    hdr = REPO / "kpp_b200" / "_gen" / f"{mech}.cuh"
+    if not hdr.exists():
+        pytest.skip("generated mechanism code not present (run the build)")
+    cxx = shutil.which("g++")
+    out = tmp_path / f"host_{mech}.so"
+    # -O without FMA contraction on x86-64: the reference's own flags
+    subprocess.run([cxx, "-O", "-fPIC", "-shared", "-std=c++17", "-I", str(REPO / "kpp_b200" / "csrc"),
+                    f'-DKPP_MECH_HEADER="{hdr}"', str(REPO / "tests" / "host_harness.cpp"),
+                    "-o", str(out)], check=True)
+    lib = ctypes.CDLL(str(out))
+    lib.host_rates.argtypes = [ctypes.c_double] * 4 + [ctypes.c_void_p] * 3
+    lib.host_fun.argtypes = [ctypes.c_void_p] * 4
+    lib.host_jac.argtypes = [ctypes.c_void_p] * 4
+    lib.host_decomp.argtypes = [ctypes.c_void_p]
+    lib.host_solve.argtypes = [ctypes.c_void_p] * 2
+    return lib
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+@pytest.mark.skipif(not ensure_built(), reason="oracle libraries not built")
+@pytest.mark.parametrize("mech", MECHS)
+def test_emitted_arithmetic_bit_identical_on_host(mech, tmp_path, golden_dir):
+    h = _host_lib(mech, tmp_path)
+    o = OracleLib(mech)
+    g = np.load(golden_dir / f"funjac_{mech}.npz")
+    for c in range(g["var"].shape[1]):
+        var = np.ascontiguousarray(g["var"][:, c])
+        fix = np.ascontiguousarray(g["fix"][:, c])
+        rc, vd, jv = np.zeros(o.nreact), np.zeros(o.nvar), np.zeros(o.lu_nonzero)
+        h.host_rates(g["temp"][c], g["cfactor"][c], g["sun"][c], g["time"][c], _p(var), _p(fix), _p(rc))
+        h.host_fun(_p(var), _p(fix), _p(rc), _p(vd))
+        h.host_jac(_p(var), _p(fix), _p(rc), _p(jv))
+        np.testing.assert_array_equal(rc, g["rconst"][:, c])
+        np.testing.assert_array_equal(vd, g["vdot"][:, c])
+        np.testing.assert_array_equal(jv, g["jvs"][:, c])
+    # LU and solve against the reference's KppDecomp / KppSolve
+    o.lib.KppDecomp.argtypes = [ctypes.c_void_p]
+    o.lib.KppSolve.argtypes = [ctypes.c_void_p] * 2
+    irow, icol, crow, diag = o.lu_pattern()
+    rng = np.random.default_rng(1)
+    for c in range(g["var"].shape[1]):
+        m = np.ascontiguousarray(-g["jvs"][:, c])
+        m[diag[:-1]] += 1.0 / (0.5 * rng.uniform(1.0, 600.0))
+        a, b = m.copy(), m.copy()
+        assert h.host_decomp(_p(a)) == o.lib.KppDecomp(_p(b))
+        np.testing.assert_array_equal(a, b)
+        x = rng.standard_normal(o.nvar)
+        xa, xb = x.copy(), x.copy()
+        h.host_solve(_p(a), _p(xa))
+        o.lib.KppSolve(_p(b), _p(xb))
+        np.testing.assert_array_equal(xa, xb)
+
+
+def test_rate_classes_are_reported(tmp_path):
+    hdr = REPO / "kpp_b200" / "_gen" / "saprc99.cuh"
+    if not hdr.exists():
+        pytest.skip("generated mechanism code not present")
+    text = hdr.read_text()
+    assert "#define KPP_RATES_DYNAMIC 0" in text
+    assert "#define KPP_RATES_SUN 30" in text
