@@ -107,8 +107,7 @@ size_t kpp_b200_workspace_bytes(int ncells);
 /* kpp_b200_rosenbrock with a caller-owned device workspace instead of the
  * library's cached one (for callers that manage device memory themselves or
  * run concurrent batches on one stream).  A workspace smaller than
- * kpp_b200_workspace_bytes(ncells) is used with fewer resident thread slots;
- * one that cannot hold one block of slots is rejected with KPP_B200_EINVAL. */
+ * kpp_b200_workspace_bytes(ncells) is rejected with KPP_B200_EINVAL. */
 int kpp_b200_rosenbrock_ws(int ncells, int ld, double *var, const double *fix,
                            const double *temp, const double *cfactor,
                            const double *sun, const double *tstart,
@@ -118,6 +117,24 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double *var, const double *fix,
                            int *istatus, double *rstatus, int *ierr,
                            void *workspace, size_t workspace_bytes,
                            void *stream);
+
+/* kpp_b200_rosenbrock on HOST arrays (same layout and meaning, all batched
+ * arrays in host memory, pinned for full copy/compute overlap): the batch is
+ * cut into chunks of `chunk` cells (0: library default) that go through
+ * host->device copy, integration and device->host copy on two streams, so the
+ * copies of one chunk overlap the integration of the other.  var, istatus,
+ * rstatus and ierr are written back to the host arrays.  Synchronous: returns
+ * when every output is in host memory.  This is the drop-in for a host model
+ * that keeps its grid in host memory and calls INTEGRATE for every cell
+ * (drv/general.c:59-76). */
+int kpp_b200_rosenbrock_host(int ncells, int ld, double *var, const double *fix,
+                             const double *temp, const double *cfactor,
+                             const double *sun, const double *tstart,
+                             const double *tend, const double *atol,
+                             const double *rtol, const int *ipar,
+                             const double *rpar, const double *hstart,
+                             int *istatus, double *rstatus, int *ierr,
+                             int chunk);
 
 /* Batched evaluation of the generated mechanism functions at time `time`
  * (the same for all cells), each exactly as FunTemplate / JacTemplate /

@@ -46,6 +46,110 @@ __device__ __forceinline__ double kpp_fall(double TEMP, double CFACTOR, float A0
   return (K0 / (1.0 + K1)) * pow((double)CF, (1.0 / (1.0 + pow((log10(K1)), 2))));
 }
 
+// ---------------------------------------------------------------------------
+// Correctly rounded cosine on [-4, 4] for Update_SUN.
+//
+// The host reference calls the C library's cos(), which returns the correctly
+// rounded result for all but a small fraction of arguments; a device cos with
+// a larger error bound would perturb SUN -- and through it the photolysis
+// rates -- at many more evaluations.  This version computes cos(x) to about
+// 2^-100 relative accuracy in double-double arithmetic and rounds once, so it
+// returns the correctly rounded value except when the exact result lies
+// within ~2^-100 of a rounding boundary.
+//   * argument reduction (Cody and Waite): x = k*pi/2 + r, |r| <= pi/4, with
+//     pi/2 split into three doubles so that r is exact to ~2^-150;
+//   * cos(r) and sin(r) by their Taylor series (16 terms each), evaluated by
+//     Horner's rule in double-double arithmetic (Dekker's exact sum and
+//     product; QD library formulation by Hida, Li and Bailey);
+//   * cos(x) = cos(r), -sin(r), -cos(r), sin(r) for k = 0, 1, 2, 3 (mod 4).
+// Constants: pi/2 and (-1)^n/(2n)!, (-1)^n/(2n+1)! rounded to double-double.
+// ---------------------------------------------------------------------------
+struct kpp_dd {
+  double hi, lo;
+};
+
+__host__ __device__ __forceinline__ double kpp_fma(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+  return __fma_rn(a, b, c);
+#else
+  return fma(a, b, c);
+#endif
+}
+
+__host__ __device__ __forceinline__ kpp_dd kpp_two_sum(double a, double b) {
+  double s = a + b;
+  double bb = s - a;
+  double e = (a - (s - bb)) + (b - bb);
+  return {s, e};
+}
+
+__host__ __device__ __forceinline__ kpp_dd kpp_fast_two_sum(double a, double b) {
+  double s = a + b;
+  return {s, b - (s - a)};
+}
+
+__host__ __device__ __forceinline__ kpp_dd kpp_dd_add(kpp_dd x, kpp_dd y) {
+  kpp_dd s = kpp_two_sum(x.hi, y.hi);
+  kpp_dd t = kpp_two_sum(x.lo, y.lo);
+  s.lo += t.hi;
+  s = kpp_fast_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return kpp_fast_two_sum(s.hi, s.lo);
+}
+
+__host__ __device__ __forceinline__ kpp_dd kpp_dd_mul(kpp_dd x, kpp_dd y) {
+  double p = x.hi * y.hi;
+  double e = kpp_fma(x.hi, y.hi, -p);
+  e += x.hi * y.lo + x.lo * y.hi;
+  return kpp_fast_two_sum(p, e);
+}
+
+__host__ __device__ inline double kpp_cos_cr(double x) {
+  const double P1 = 1.5707963267948966, P2 = 6.123233995736766e-17,
+               P3 = -1.4973849048591698e-33;
+  const double kc[17][2] = {
+      {1.0, 0.0}, {-0.5, 0.0}, {0.041666666666666664, 2.3129646346357427e-18},
+      {-0.001388888888888889, 5.300543954373577e-20}, {2.48015873015873e-05, 2.1511947866775882e-23},
+      {-2.755731922398589e-07, -2.3767714622250297e-23}, {2.08767569878681e-09, -1.20734505911326e-25},
+      {-1.1470745597729725e-11, -2.0655512752830745e-28}, {4.779477332387385e-14, 4.399205485834081e-31},
+      {-1.5619206968586225e-16, -1.1910679660273754e-32}, {4.110317623312165e-19, 1.4412973378659527e-36},
+      {-8.896791392450574e-22, 7.911402614872376e-38}, {1.6117375710961184e-24, -3.6846573564509766e-41},
+      {-2.4795962632247976e-27, 1.2953730964765229e-43}, {3.279889237069838e-30, 1.5117542744029879e-46},
+      {-3.7699876288159054e-33, -2.5870347832750324e-49}, {3.8003907548547434e-36, 1.7457158024652518e-52}};
+  const double ks[17][2] = {
+      {1.0, 0.0}, {-0.16666666666666666, -9.25185853854297e-18},
+      {0.008333333333333333, 1.1564823173178714e-19}, {-0.0001984126984126984, -1.7209558293420705e-22},
+      {2.7557319223985893e-06, -1.858393274046472e-22}, {-2.505210838544172e-08, 1.448814070935912e-24},
+      {1.6059043836821613e-10, 1.2585294588752098e-26}, {-7.647163731819816e-13, -7.03872877733453e-30},
+      {2.8114572543455206e-15, 1.6508842730861433e-31}, {-8.22063524662433e-18, -2.2141894119604265e-34},
+      {1.9572941063391263e-20, -1.3643503830087908e-36}, {-3.868170170630684e-23, 8.843177655482344e-40},
+      {6.446950284384474e-26, -1.9330404233703465e-42}, {-9.183689863795546e-29, -1.4303150396787322e-45},
+      {1.1309962886447716e-31, 1.0498015412959506e-47}, {-1.216125041553518e-34, -5.586290567888806e-51},
+      {1.151633562077195e-37, -6.09957445788454e-54}};
+  double kf = rint(x * 0.6366197723675814);
+  int k = (int)kf;
+  kpp_dd r = kpp_two_sum(x, -kf * P1);  // k*P1 is exact for |k| <= 3
+  r = kpp_dd_add(r, {-kf * P2, 0.0});
+  r = kpp_dd_add(r, {-kf * P3, 0.0});
+  kpp_dd r2 = kpp_dd_mul(r, r);
+  const bool use_sin = (k & 1) != 0;
+  kpp_dd p = use_sin ? kpp_dd{ks[16][0], ks[16][1]} : kpp_dd{kc[16][0], kc[16][1]};
+  for (int n = 15; n >= 0; n--) {
+    kpp_dd c = use_sin ? kpp_dd{ks[n][0], ks[n][1]} : kpp_dd{kc[n][0], kc[n][1]};
+    p = kpp_dd_add(kpp_dd_mul(p, r2), c);
+  }
+  if (use_sin) p = kpp_dd_mul(p, r);
+  double v = p.hi + p.lo;
+  int q = k & 3;
+  return (q == 1 || q == 2) ? -v : v;
+}
+
+// The cosine of Update_SUN (the host harness of the tests substitutes the C
+// library's to compare generated code bit for bit with the reference).
+#ifndef KPP_SUN_COS
+#define KPP_SUN_COS kpp_cos_cr
+#endif
+
 // SUN in [0,1] from the model time: a cosine-shaped day between 4.5 h and
 // 19.5 h local time, 0 at night (util/UpdateSun.c:1-20).
 __device__ __forceinline__ double kpp_update_sun(double TIME) {
@@ -57,7 +161,7 @@ __device__ __forceinline__ double kpp_update_sun(double TIME) {
     double Ttmp = (2.0 * Tlocal - SunRise - SunSet) / (SunSet - SunRise);
     if (Ttmp > 0) Ttmp = Ttmp * Ttmp;
     else Ttmp = -Ttmp * Ttmp;
-    return (1.0 + cos(PI * Ttmp)) / 2.0;
+    return (1.0 + KPP_SUN_COS(PI * Ttmp)) / 2.0;
   }
   return 0.0;
 }

@@ -199,13 +199,17 @@ struct Stats {
   int nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng;
 };
 
-// A per-cell array of a thread slot inside the scratch buffer: element i at
-// p[i * s].  Consecutive slots are consecutive doubles, so a warp touching
-// the same element of 32 cells issues one coalesced 256-byte access.
+// Scratch layout: element i of a per-cell work array of thread slot t lives
+// at base[(offset_of_array + i) * kSlotStride + t].  Consecutive slots are
+// consecutive doubles, so a warp touching the same element of 32 cells issues
+// one coalesced 256-byte access.  The stride is a compile-time constant: every
+// access is then base + constant + slot, which lets the compiler prove that
+// different elements do not alias and keep, reorder and batch its loads.
+constexpr long kSlotStride = 1L << 17;  // thread slots of the layout (>= resident threads)
+
 struct Strided {
   double* p;
-  long s;
-  __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * s]; }
+  __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * kSlotStride]; }
 };
 
 // Doubles of work storage one thread slot needs in the scratch layout.
@@ -218,10 +222,10 @@ constexpr long kScratchPerSlot = (long)LU_NZ + (long)kMaxStages * NVAR + 6L * NV
 struct Work {
   Strided y, ynew, fcn0, fcn, dfdt, yerr, jvs, rconst, a, b;
   Strided k[kMaxStages];
-  __device__ __forceinline__ Work(double* base, long nslots, long slot) {
+  __device__ __forceinline__ Work(double* base, long, long slot) {
     long off = 0;
     auto take = [&](long n) {
-      Strided v{base + off * nslots + slot, nslots};
+      Strided v{base + off * kSlotStride + slot};
       off += n;
       return v;
     };
@@ -624,14 +628,21 @@ __global__ void __launch_bounds__(128) fun_jac_kernel(const EvalArgs a) {
   }
 }
 
+// A batched array with a run-time leading dimension (the ABI layout).
+struct StridedLd {
+  double* p;
+  long s;
+  __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * s]; }
+};
+
 __global__ void __launch_bounds__(128) decomp_solve_kernel(int ncells, int ld, double* jvs_g,
                                                            double* x_g, int* ising) {
   const int cell = blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= ncells) return;
-  Strided jvs{jvs_g + cell, ld};
+  StridedLd jvs{jvs_g + cell, ld};
   ising[cell] = kpp_decomp(jvs);
   if (x_g) {
-    Strided x{x_g + cell, ld};
+    StridedLd x{x_g + cell, ld};
     kpp_solve(jvs, x);
   }
 }
@@ -666,11 +677,13 @@ long slots_for(int ncells) {
     res = it->second;
   }
   long want = ((long)ncells + kBlock - 1) / kBlock * kBlock;
+  if (res > kSlotStride) res = kSlotStride;
   return want < res ? want : res;
 }
 
-size_t scratch_bytes(long nslots) {
-  return kUsesScratch ? (size_t)kScratchPerSlot * (size_t)nslots * sizeof(double) : 0;
+// The scratch layout always spans kSlotStride slots (its stride is fixed).
+size_t scratch_bytes(long) {
+  return kUsesScratch ? (size_t)kScratchPerSlot * (size_t)kSlotStride * sizeof(double) : 0;
 }
 
 // Library-managed work buffers, one per (device, stream), grown on demand and
@@ -741,6 +754,131 @@ int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
   a.nslots = 0;
   if (ipar) std::memcpy(a.ipar, ipar, sizeof a.ipar);
   if (rpar) std::memcpy(a.rpar, rpar, sizeof a.rpar);
+  return KPP_B200_OK;
+}
+
+
+// ---- host-buffer pipeline ---------------------------------------------------
+// Device buffers of one chunk (ABI layout, leading dimension = chunk size).
+struct ChunkBuffers {
+  long cap = 0;
+  double *var = nullptr, *fix = nullptr, *temp = nullptr, *cfactor = nullptr, *sun = nullptr;
+  double *tstart = nullptr, *tend = nullptr, *hstart = nullptr, *rstatus = nullptr;
+  double *atol = nullptr, *rtol = nullptr;
+  int *istatus = nullptr, *ierr = nullptr;
+  cudaStream_t stream = nullptr;
+
+  void release() {
+    for (void* p : {(void*)var, (void*)fix, (void*)temp, (void*)cfactor, (void*)sun,
+                    (void*)tstart, (void*)tend, (void*)hstart, (void*)rstatus, (void*)atol,
+                    (void*)rtol, (void*)istatus, (void*)ierr})
+      if (p) cudaFree(p);
+    *this = ChunkBuffers{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, stream};
+  }
+
+  int ensure(long n) {
+    if (!stream) {
+      cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_fail("cudaStreamCreate", e);
+    }
+    if (cap >= n) return KPP_B200_OK;
+    release();
+    size_t d = sizeof(double);
+    struct { void** p; size_t bytes; } want[] = {
+        {(void**)&var, (size_t)NVAR * n * d}, {(void**)&fix, (size_t)(NFIX_TRUE > 0 ? NFIX_TRUE : 1) * n * d},
+        {(void**)&temp, n * d}, {(void**)&cfactor, n * d}, {(void**)&sun, n * d},
+        {(void**)&tstart, n * d}, {(void**)&tend, n * d}, {(void**)&hstart, n * d},
+        {(void**)&rstatus, 2 * n * d}, {(void**)&atol, NVAR * d}, {(void**)&rtol, NVAR * d},
+        {(void**)&istatus, 8 * n * sizeof(int)}, {(void**)&ierr, n * sizeof(int)}};
+    for (auto& w : want) {
+      cudaError_t e = cudaMalloc(w.p, w.bytes);
+      if (e != cudaSuccess) {
+        release();
+        return cuda_fail("cudaMalloc(chunk buffers)", e);
+      }
+    }
+    cap = n;
+    return KPP_B200_OK;
+  }
+};
+
+// rows x cols block of a host ABI array (leading dimension ld, first column c0)
+// to/from a device array with leading dimension dld.
+inline cudaError_t copy_rows(void* dst, long dld, const void* src, long sld, long c0, long cols,
+                             long rows, size_t elem, cudaMemcpyKind kind, cudaStream_t s,
+                             bool src_offset) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  const char* sp = (const char*)src + (src_offset ? c0 * elem : 0);
+  char* dp = (char*)dst + (src_offset ? 0 : c0 * elem);
+  return cudaMemcpy2DAsync(dp, dld * elem, sp, sld * elem, cols * elem, rows, kind, s);
+}
+
+int host_pipeline(int ncells, int ld, double* var, const double* fix, const double* temp,
+                  const double* cfactor, const double* sun, const double* tstart,
+                  const double* tend, const double* atol, const double* rtol, const int* ipar,
+                  const double* rpar, const double* hstart, int* istatus, double* rstatus,
+                  int* ierr, int chunk) {
+  static std::mutex mu;
+  static std::map<int, ChunkBuffers[2]> per_device;
+  std::lock_guard<std::mutex> lock(mu);  // one host pipeline per process at a time
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  long csz = chunk > 0 ? chunk : (1L << 18);
+  if (csz > ncells) csz = ncells;
+  ChunkBuffers* bufs = per_device[dev];
+  const int ntol = (ipar[1] == 0) ? NVAR : 1;
+  for (int b = 0; b < 2; b++) {
+    int rc = bufs[b].ensure(csz);
+    if (rc != KPP_B200_OK) return rc;
+    e = cudaMemcpyAsync(bufs[b].atol, atol, ntol * sizeof(double), cudaMemcpyHostToDevice,
+                        bufs[b].stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(bufs[b].rtol, rtol, ntol * sizeof(double), cudaMemcpyHostToDevice,
+                          bufs[b].stream);
+    if (e != cudaSuccess) return cuda_fail("tolerance copy", e);
+  }
+  const auto H2D = cudaMemcpyHostToDevice;
+  const auto D2H = cudaMemcpyDeviceToHost;
+  long nchunks = ((long)ncells + csz - 1) / csz;
+  for (long c = 0; c < nchunks; c++) {
+    ChunkBuffers& B = bufs[c & 1];
+    cudaStream_t s = B.stream;
+    long c0 = c * csz, n = ((long)ncells - c0 < csz) ? (long)ncells - c0 : csz;
+    e = copy_rows(B.var, csz, var, ld, c0, n, NVAR, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess && NFIX_TRUE > 0)
+      e = copy_rows(B.fix, csz, fix, ld, c0, n, NFIX_TRUE, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess) e = copy_rows(B.temp, csz, temp, ld, c0, n, 1, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess && cfactor)
+      e = copy_rows(B.cfactor, csz, cfactor, ld, c0, n, 1, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess && sun) e = copy_rows(B.sun, csz, sun, ld, c0, n, 1, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess) e = copy_rows(B.tstart, csz, tstart, ld, c0, n, 1, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess) e = copy_rows(B.tend, csz, tend, ld, c0, n, 1, sizeof(double), H2D, s, true);
+    if (e == cudaSuccess && hstart)
+      e = copy_rows(B.hstart, csz, hstart, ld, c0, n, 1, sizeof(double), H2D, s, true);
+    if (e != cudaSuccess) return cuda_fail("host->device copy", e);
+
+    LaunchArgs a;
+    fill_args(a, (int)n, (int)csz, B.var, B.fix, B.temp, cfactor ? B.cfactor : nullptr,
+              sun ? B.sun : nullptr, B.tstart, B.tend, B.atol, B.rtol, ipar, rpar,
+              hstart ? B.hstart : nullptr, B.istatus, B.rstatus, B.ierr);
+    a.nslots = slots_for((int)n);
+    int rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+    if (rc != KPP_B200_OK) return rc;
+    rc = launch_rosenbrock(a, s);
+    if (rc != KPP_B200_OK) return rc;
+
+    e = copy_rows(var, ld, B.var, csz, c0, n, NVAR, sizeof(double), D2H, s, false);
+    if (e == cudaSuccess) e = copy_rows(istatus, ld, B.istatus, csz, c0, n, 8, sizeof(int), D2H, s, false);
+    if (e == cudaSuccess) e = copy_rows(rstatus, ld, B.rstatus, csz, c0, n, 2, sizeof(double), D2H, s, false);
+    if (e == cudaSuccess) e = copy_rows(ierr, ld, B.ierr, csz, c0, n, 1, sizeof(int), D2H, s, false);
+    if (e != cudaSuccess) return cuda_fail("device->host copy", e);
+  }
+  for (int b = 0; b < 2; b++) {
+    e = cudaStreamSynchronize(bufs[b].stream);
+    if (e != cudaSuccess) return cuda_fail("cudaStreamSynchronize", e);
+  }
   return KPP_B200_OK;
 }
 
@@ -822,14 +960,25 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double* var, const double* fix, c
   if (rc != KPP_B200_OK || ncells == 0) return rc;
   a.nslots = slots_for(ncells);
   if (kUsesScratch) {
-    long fit = (long)(workspace_bytes / ((size_t)kScratchPerSlot * sizeof(double)));
-    fit = fit / kBlock * kBlock;
-    if (!workspace || fit < kBlock)
-      return fail(KPP_B200_EINVAL, "workspace smaller than one block of thread slots");
-    if (fit < a.nslots) a.nslots = fit;
+    if (!workspace || workspace_bytes < scratch_bytes(a.nslots))
+      return fail(KPP_B200_EINVAL, "workspace smaller than kpp_b200_workspace_bytes()");
     a.scratch = (double*)workspace;
   }
   return launch_rosenbrock(a, (cudaStream_t)stream);
+}
+
+int kpp_b200_rosenbrock_host(int ncells, int ld, double* var, const double* fix,
+                             const double* temp, const double* cfactor, const double* sun,
+                             const double* tstart, const double* tend, const double* atol,
+                             const double* rtol, const int* ipar, const double* rpar,
+                             const double* hstart, int* istatus, double* rstatus, int* ierr,
+                             int chunk) {
+  LaunchArgs chk;
+  int rc = fill_args(chk, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol,
+                     ipar, rpar, hstart, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  return host_pipeline(ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, ipar,
+                       rpar, hstart, istatus, rstatus, ierr, chunk);
 }
 
 int kpp_b200_fun_jac(int ncells, int ld, const double* var, const double* fix,

@@ -89,6 +89,7 @@ class Mechanism:
         ros = [ctypes.c_int, ctypes.c_int] + [_vp] * 9 + [_c_int_p, _c_double_p, _vp, _vp, _vp, _vp]
         L.kpp_b200_rosenbrock.argtypes = ros + [_vp]
         L.kpp_b200_rosenbrock_ws.argtypes = ros + [_vp, ctypes.c_size_t, _vp]
+        L.kpp_b200_rosenbrock_host.argtypes = ros + [ctypes.c_int]
         L.kpp_b200_fun_jac.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 4
         L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
 
@@ -162,6 +163,43 @@ class Mechanism:
                 _vp(s.cuda_stream)))
         else:
             self._check(self.lib.kpp_b200_rosenbrock(*args, _vp(s.cuda_stream)))
+        return out
+
+    @staticmethod
+    def _host(t, dtype, name):
+        if t is None:
+            return None
+        if not isinstance(t, torch.Tensor) or t.is_cuda:
+            raise KppError(f"{name} must be a host (CPU) tensor")
+        if t.dtype != dtype or not t.is_contiguous():
+            raise KppError(f"{name} must be a contiguous {dtype} tensor")
+        return t
+
+    def rosenbrock_host(self, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar,
+                        cfactor=None, sun=None, hstart=None, ncells=None, out=None,
+                        chunk: int = 0) -> RosenbrockResult:
+        """Batched Rosenbrock on host tensors (kpp_b200_rosenbrock_host): chunked
+        copies overlapped with the integration; synchronous.  Pinned tensors
+        give full overlap."""
+        f64, i32 = torch.float64, torch.int32
+        self._host(var, f64, "var")
+        ld = var.shape[1]
+        n = ld if ncells is None else ncells
+        for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                      (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun"),
+                      (hstart, "hstart")):
+            self._host(t, f64, nm)
+        if out is None:
+            pin = torch.cuda.is_available()
+            out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, pin_memory=pin),
+                                   istatus=torch.empty(8, ld, dtype=i32, pin_memory=pin),
+                                   rstatus=torch.empty(2, ld, dtype=f64, pin_memory=pin))
+        ip = (ctypes.c_int * 20)(*[int(x) for x in ipar])
+        rp = (ctypes.c_double * 20)(*[float(x) for x in rpar])
+        self._check(self.lib.kpp_b200_rosenbrock_host(
+            n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
+            _ptr(tend), _ptr(atol), _ptr(rtol), ip, rp, _ptr(hstart), _ptr(out.istatus),
+            _ptr(out.rstatus), _ptr(out.ierr), int(chunk)))
         return out
 
     def fun_jac(self, var, fix, temp, time: float, cfactor=None, sun=None,

@@ -14,7 +14,7 @@
  * FunTemplate / JacTemplate (Update_SUN + Update_RCONST + Fun / Jac_SP,
  * int/rosenbrock.c:1257-1296) and the generated LU_* sparsity arrays.
  *
- * How it is pinned: tests/test_oracle_ref.py runs this restatement and the
+ * How it is pinned: tests/test_oracle_pin.py runs this restatement and the
  * reference's own Rosenbrock (oracle/refkpp/batch_driver.c) on the same cells
  * and requires bit-identical results, statistics and error codes.
  *
@@ -42,6 +42,20 @@
 void FunTemplate(double T, double Y[], double Ydot[]);
 void JacTemplate(double T, double Y[], double Jcb[]);
 extern double kppref_sun_override;
+
+/* Test knob (0 = off, the default, bit-identical to the reference): move the
+ * result of pow(Err, 1/ELO) in the step-size controller by one ulp up (1) or
+ * down (-1), to measure how far a last-ulp difference of pow() moves the
+ * results. */
+static int kppor_pow_ulps = 0;
+void kppor_set_pow_ulps(int u) { kppor_pow_ulps = u; }
+
+static double or_pow_step(double err, double e) {
+  double v = pow(err, e);
+  if (kppor_pow_ulps > 0) v = nextafter(v, HUGE_VAL);
+  if (kppor_pow_ulps < 0) v = nextafter(v, -HUGE_VAL);
+  return v;
+}
 
 typedef struct {
   int nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng;
@@ -370,7 +384,7 @@ static int or_integrator(double *y, double tstart, double tend, const double *at
       for (j = 1; j <= m->S; j++) or_axpy(NVAR, m->E[j - 1], &k[NVAR * (j - 1)], yerr);
       err = or_error_norm(y, ynew, yerr, atol, rtol, vectortol);
 
-      fac = OR_MIN(facmax, OR_MAX(facmin, facsafe / pow(err, OR_ONE / m->ELO)));
+      fac = OR_MIN(facmax, OR_MAX(facmin, facsafe / or_pow_step(err, OR_ONE / m->ELO)));
       hnew = h * fac;
 
       st->nstp++;

@@ -10,7 +10,7 @@ batches and stores inputs and outputs:
   funjac_<mech>.npz       rate constants, Fun and Jac_SP of a few cells
   integrate_<mech>.npz    chained chemistry steps of a small batch: inputs,
                           VAR after every step, ISTATUS, RSTATUS and IERR, and
-                          var_alt [step, 3, NVAR, cells]: the same steps by the
+                          var_alt [step, 5, NVAR, cells]: the same steps by the
                           reference under other valid last-ulp roundings
                           (oracle_lib.alternates)
 
@@ -86,7 +86,8 @@ def integrate_chain(o: OracleLib, wl: workloads.Workload, nsteps: int) -> dict:
                                           wl.ipar, wl.rpar, cfactor=wl.cfactor, sun=wl.sun,
                                           hstart=hstart, which="ref")
         # the same step by the reference under other valid last-ulp roundings
-        # (FMA contraction; SUN one ulp up / down), which measures how far the
+        # (FMA contraction; SUN one ulp up / down; the
+        # step controller's pow() one ulp up / down), which measures how far the
         # result itself moves under last-ulp perturbations
         va = alternates(o.mech, prev, wl.fix, wl.temp, t0, t1, wl.atol, wl.rtol, wl.ipar,
                         wl.rpar, cfactor=wl.cfactor, sun=wl.sun, hstart=hstart)

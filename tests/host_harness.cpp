@@ -11,9 +11,15 @@
 #include <cmath>
 using std::cos;
 using std::exp;
+using std::fma;
 using std::log10;
 using std::pow;
+using std::rint;
+#define KPP_SUN_COS cos
 #include "kpp_ratelaws.cuh"
+
+// the device cosine of Update_SUN, for its own test
+extern "C" double host_cos_cr(double x) { return kpp_cos_cr(x); }
 #include KPP_MECH_HEADER
 
 extern "C" {

@@ -105,9 +105,9 @@ class OracleLib:
 def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, cfactor=None,
                sun=None, hstart=None):
     """VAR after the same integration by the reference under other valid
-    last-ulp roundings: compiled with FMA contraction, and with SUN moved by
-    one ulp up and down at every evaluation (the size of a cos() difference
-    in Update_SUN).  Their spread around the reference measures how strongly
+    last-ulp roundings: compiled with FMA contraction; SUN moved by one ulp up
+    and down at every evaluation (the size of a cos() difference in
+    Update_SUN); and pow() of the step-size controller one ulp up and down.  Their spread around the reference measures how strongly
     each entry amplifies last-ulp perturbations."""
     out = []
     o3 = OracleLib(mech, "_O3")
@@ -121,4 +121,13 @@ def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, 
                                    cfactor=cfactor, sun=sun, hstart=hstart)[0])
         finally:
             o.set_sun_ulps(0)
+    # pow() of the step-size controller one ulp up / down (the restatement,
+    # bit-identical to the reference with the knob off)
+    for u in (1, -1):
+        o.lib.kppor_set_pow_ulps(ctypes.c_int(u))
+        try:
+            out.append(o.integrate(var, fix, temp, tstart, tend, atol, rtol, ipar, rpar,
+                                   cfactor=cfactor, sun=sun, hstart=hstart, which="port")[0])
+        finally:
+            o.lib.kppor_set_pow_ulps(ctypes.c_int(0))
     return np.stack(out)

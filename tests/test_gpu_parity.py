@@ -218,3 +218,23 @@ def test_singular_pivot_detected():
     ising = m.decomp_solve(jvs)
     torch.cuda.synchronize()
     assert ising.cpu().tolist() == [0, 3, 0, 1]
+
+
+def test_host_entry_matches_device_entry():
+    """kpp_b200_rosenbrock_host (chunked, two streams) gives the device entry's
+    results bit for bit, for chunks that do not divide the batch."""
+    m = load("saprc99")
+    wl = workloads.for_mechanism(m, "saprc99", 1000, seed=21)
+    t0, t1 = wl.step_bounds(0)
+    var = dev(wl.var)
+    r = m.rosenbrock(var, dev(wl.fix), dev(wl.temp), dev(t0), dev(t1), dev(wl.atol), dev(wl.rtol),
+                     wl.ipar, wl.rpar, cfactor=dev(wl.cfactor), sun=dev(wl.sun))
+    torch.cuda.synchronize()
+    h = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hvar = h(wl.var)
+    rh = m.rosenbrock_host(hvar, h(wl.fix), h(wl.temp), h(t0), h(t1), h(wl.atol), h(wl.rtol),
+                           wl.ipar, wl.rpar, cfactor=h(wl.cfactor), sun=h(wl.sun), chunk=300)
+    np.testing.assert_array_equal(hvar.numpy(), var.cpu().numpy())
+    np.testing.assert_array_equal(rh.istatus.numpy(), r.istatus.cpu().numpy())
+    np.testing.assert_array_equal(rh.rstatus.numpy(), r.rstatus.cpu().numpy())
+    np.testing.assert_array_equal(rh.ierr.numpy(), r.ierr.cpu().numpy())
