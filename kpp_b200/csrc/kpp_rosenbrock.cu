@@ -199,17 +199,19 @@ struct Stats {
   int nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng;
 };
 
-// Scratch layout: element i of a per-cell work array of thread slot t lives
-// at base[(offset_of_array + i) * kSlotStride + t].  Consecutive slots are
-// consecutive doubles, so a warp touching the same element of 32 cells issues
-// one coalesced 256-byte access.  The stride is a compile-time constant: every
-// access is then base + constant + slot, which lets the compiler prove that
-// different elements do not alias and keep, reorder and batch its loads.
-constexpr long kSlotStride = 1L << 17;  // thread slots of the layout (>= resident threads)
+// Scratch layout, blocked by warp: the 32 thread slots of a warp own one
+// contiguous block, and element i of a per-cell work array of lane l sits at
+// block[(offset_of_array + i) * 32 + l].  A warp touching the same element of
+// its 32 cells issues one coalesced 256-byte access; every access is the
+// lane's block pointer plus a compile-time constant below 1 MB, so it fits
+// the load/store immediate offset, and the compiler can prove that different
+// elements do not alias and keep, reorder and batch its loads.
+constexpr long kSlotStride = 1L << 17;  // thread slots the layout holds (>= resident threads)
+constexpr int kLanes = 32;
 
 struct Strided {
   double* p;
-  __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * kSlotStride]; }
+  __device__ __forceinline__ double& operator[](int i) const { return p[i * kLanes]; }
 };
 
 // Doubles of work storage one thread slot needs in the scratch layout.
@@ -223,9 +225,10 @@ struct Work {
   Strided y, ynew, fcn0, fcn, dfdt, yerr, jvs, rconst, a, b;
   Strided k[kMaxStages];
   __device__ __forceinline__ Work(double* base, long, long slot) {
+    double* block = base + (slot / kLanes) * kScratchPerSlot * kLanes + (slot % kLanes);
     long off = 0;
     auto take = [&](long n) {
-      Strided v{base + off * kSlotStride + slot};
+      Strided v{block + off * kLanes};
       off += n;
       return v;
     };
@@ -533,9 +536,22 @@ template <int M>
 int occupancy_method();
 
 #if KPP_PART >= 1
+// Resident blocks per SM the compiler must allow (bounds the registers per
+// thread: 65536 / (128 * KPP_MIN_BLOCKS)); 0 leaves the choice to ptxas.
+// 8 blocks (64 registers) measured fastest for saprc99 on B200.
+#ifndef KPP_MIN_BLOCKS
+#define KPP_MIN_BLOCKS 8
+#endif
+
 // One thread slot integrates cells slot, slot + nslots, ... (grid-stride).
 template <int METHOD>
-__global__ void __launch_bounds__(128) rosenbrock_kernel(const LaunchArgs a) {
+__global__ void
+#if KPP_MIN_BLOCKS > 0
+__launch_bounds__(128, KPP_MIN_BLOCKS)
+#else
+__launch_bounds__(128)
+#endif
+rosenbrock_kernel(const LaunchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long ld = a.ld;
   Work w(a.scratch, a.nslots, slot);
