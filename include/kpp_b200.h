@@ -118,6 +118,30 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double *var, const double *fix,
                            void *workspace, size_t workspace_bytes,
                            void *stream);
 
+/* Allocation-free kpp_b200_rosenbrock.  No counterpart in the reference.
+ * For callers that cannot allocate device memory -- code running where
+ * cudaMalloc is not allowed (inside a stream capture that must not allocate,
+ * a host model with a fixed device-memory budget, or a library that is handed
+ * only its inputs and outputs).  The caller still passes every input and
+ * output; the work arrays live in a fixed device array inside the library,
+ * sized for at most 1024 cells per call (about 21 MB for saprc99, reserved on
+ * every GPU that loads the library, until exit).  Larger batches are rejected
+ * with KPP_B200_EINVAL; split them into calls of at most 1024 cells.
+ * The first call on a device looks up that array's device address, so make it
+ * before any stream capture.  No memory is allocated or freed by any call.
+ * Every call uses the same array: calls that overlap on the GPU (concurrent
+ * streams) race on it, so issue them on one stream or serialise them.  No
+ * state carries over between calls: each call writes every work element
+ * before reading it, so nothing needs clearing. */
+int kpp_b200_rosenbrock_static(int ncells, int ld, double *var, const double *fix,
+                               const double *temp, const double *cfactor,
+                               const double *sun, const double *tstart,
+                               const double *tend, const double *atol,
+                               const double *rtol, const int *ipar,
+                               const double *rpar, const double *hstart,
+                               int *istatus, double *rstatus, int *ierr,
+                               void *stream);
+
 /* kpp_b200_rosenbrock on HOST arrays (same layout and meaning, all batched
  * arrays in host memory, pinned for full copy/compute overlap): the batch is
  * cut into chunks of `chunk` cells (0: library default) that go through

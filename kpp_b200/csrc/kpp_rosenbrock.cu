@@ -774,6 +774,43 @@ int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
 }
 
 
+// ---- allocation-free variant -------------------------------------------------
+// For callers that cannot allocate device memory: the work arrays of the
+// allocation-free entry live in this file-scope device array, sized for
+// kStaticMaxCells cells (one thread slot each, warp-blocked layout).  Every GPU
+// that loads the library holds it until the process exits.  Host code must not
+// use the array's name as a device address (on the host it names a host-side
+// stand-in); static_scratch() obtains the device address per device.
+constexpr int kStaticMaxCells = 1024;
+static_assert(kStaticMaxCells % kBlock == 0, "whole blocks of thread slots");
+#if defined(KPP_SCRATCH)
+static __device__ __align__(256) double g_static_scratch[(size_t)kScratchPerSlot * kStaticMaxCells];
+#endif
+
+// Device address of g_static_scratch on the current device (nullptr for
+// mechanisms whose work arrays are thread-local).  Looked up with
+// cudaGetSymbolAddress on the first call per device, with that device current.
+int static_scratch(double** out) {
+  *out = nullptr;
+#if defined(KPP_SCRATCH)
+  static std::mutex mu;
+  static std::map<int, double*> addr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = addr.find(dev);
+  if (it == addr.end()) {
+    double* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress(g_static_scratch)", e);
+    it = addr.emplace(dev, p).first;
+  }
+  *out = it->second;
+#endif
+  return KPP_B200_OK;
+}
+
 // ---- host-buffer pipeline ---------------------------------------------------
 // Device buffers of one chunk (ABI layout, leading dimension = chunk size).
 struct ChunkBuffers {
@@ -980,6 +1017,29 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double* var, const double* fix, c
       return fail(KPP_B200_EINVAL, "workspace smaller than kpp_b200_workspace_bytes()");
     a.scratch = (double*)workspace;
   }
+  return launch_rosenbrock(a, (cudaStream_t)stream);
+}
+
+int kpp_b200_rosenbrock_static(int ncells, int ld, double* var, const double* fix,
+                               const double* temp, const double* cfactor, const double* sun,
+                               const double* tstart, const double* tend, const double* atol,
+                               const double* rtol, const int* ipar, const double* rpar,
+                               const double* hstart, int* istatus, double* rstatus, int* ierr,
+                               void* stream) {
+  LaunchArgs a;
+  int rc = fill_args(a, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, ipar,
+                     rpar, hstart, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  if (ncells > kStaticMaxCells) {
+    std::snprintf(g_last_error, sizeof g_last_error,
+                  "kpp_b200_rosenbrock_static: %d cells exceed its maximum of %d cells per call",
+                  ncells, kStaticMaxCells);
+    return KPP_B200_EINVAL;
+  }
+  // one thread slot per cell, in whole blocks: at most kStaticMaxCells slots
+  a.nslots = ((long)ncells + kBlock - 1) / kBlock * kBlock;
+  rc = static_scratch(&a.scratch);
+  if (rc != KPP_B200_OK) return rc;
   return launch_rosenbrock(a, (cudaStream_t)stream);
 }
 
