@@ -189,6 +189,8 @@ def run_cuda_arm(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
+    mech.set_kernel(args.kernel)
+    kernel = mech.kernel()
     wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=workloads.SEED_EVAL + rank)
     n = wl.ncells
     D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -337,9 +339,10 @@ def run_cuda_arm(args, rank, world, local_rank):
                    "mode": args.mode,
                    "cells_per_gpu": n, "chemistry_step_s": wl.dt, "method": "rodas3",
                    "scheduler": "plain", "parallelism": f"cell shards x{world}",
+                   "kernel": {"thread": "thread per cell", "warp": "warp per cell"}[kernel],
                    "l2": "inputs larger than L2 (VAR alone %d MB)" % (wl.var.nbytes >> 20)},
         "impl": "kpp_b200",
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (2 if kernel == "warp" else 1),
         "stats": {"internal_steps_per_cell_step": nstp / (n * args.steps),
                   "rejected_per_cell_step": nrej / (n * args.steps),
                   "ierr_ok_fraction": float((ierr == 1).mean()),
@@ -371,6 +374,7 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--kernel", choices=["auto", "thread", "warp"], default="auto")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

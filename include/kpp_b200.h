@@ -177,6 +177,16 @@ int kpp_b200_fun_jac(int ncells, int ld, const double *var, const double *fix,
 int kpp_b200_decomp_solve(int ncells, int ld, double *jvs, double *x,
                           int *ising, void *stream);
 
+/* Kernel used by the Rosenbrock entries (process-wide): 0 automatic (the
+ * default), 1 one thread per cell with the work set in device memory, 2 one
+ * warp per cell with the work set in shared memory (mechanisms whose work set
+ * is in device memory and fits shared memory; others keep kernel 1).  Both
+ * kernels give bit-identical results.  Automatic selects kernel 1.  No
+ * counterpart in the reference.
+ * kpp_b200_get_kernel returns the kernel in effect (1 or 2). */
+int kpp_b200_set_kernel(int which);
+int kpp_b200_get_kernel(void);
+
 /* Text of the last error of this thread's last failing call. */
 const char *kpp_b200_last_error(void);
 

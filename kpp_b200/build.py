@@ -136,7 +136,8 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> 
     defines = [f'-DKPP_MECH_HEADER="{header}"']
     if meta["lu_nonzero"] >= SCRATCH_LU_NONZERO:
         defines.append("-DKPP_SCRATCH")
-    srcs = [CSRC / "kpp_rosenbrock.cu", CSRC / "kpp_ratelaws.cuh", header, INCLUDE / "kpp_b200.h"]
+    srcs = [CSRC / "kpp_rosenbrock.cu", CSRC / "kpp_ratelaws.cuh", CSRC / "kpp_warp.cuh", header,
+            INCLUDE / "kpp_b200.h"]
     digest = _hash_files(srcs, " ".join(ARCH + NVCC_FLAGS + defines))
     lib = library_path(mech)
     stamp = objdir / "lib.stamp"

@@ -191,6 +191,7 @@ struct LaunchArgs {
   int* ierr;
   double* scratch;  // work arrays of every thread slot (scratch layout), or null
   long nslots;      // thread slots of the grid = stride of the scratch arrays
+  size_t scratch_doubles;  // capacity of `scratch`
   int ipar[20];
   double rpar[20];
 };
@@ -534,6 +535,12 @@ template <int M>
 int launch_method(LaunchArgs& a, int grid, cudaStream_t s);
 template <int M>
 int occupancy_method();
+// The warp-cooperative kernel of method M (one warp per cell in shared
+// memory); `rates` holds the cells' fixed rate constants [NREACT][rates_ld].
+template <int M>
+int launch_method_warp(LaunchArgs& a, const double* rates, long rates_ld, cudaStream_t s);
+// Shared memory per cell of the warp kernel (bytes).
+size_t warp_smem_bytes();
 
 #if KPP_PART >= 1
 // Resident blocks per SM the compiler must allow (bounds the registers per
@@ -600,9 +607,75 @@ int occupancy_method() {
 template int launch_method<KPP_PART>(LaunchArgs&, int, cudaStream_t);
 template int occupancy_method<KPP_PART>();
 
+#include "kpp_warp.cuh"
+
+template <int M>
+int launch_method_warp(LaunchArgs& a, const double* rates, long rates_ld, cudaStream_t s) {
+  static int grid_cap = 0;  // resident warps on this device (one per block)
+  if (grid_cap == 0) {
+    int dev = 0, sms = 1, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(warpk::kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)warpk::kSmemBytes);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warpk::kernel<M>, 32,
+                                                      warpk::kSmemBytes) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    grid_cap = sms * per_sm;
+  }
+  const int grid = a.ncells < grid_cap ? a.ncells : grid_cap;
+  warpk::kernel<M><<<grid, 32, warpk::kSmemBytes, s>>>(a, rates, rates_ld);
+  return check_launch("warp rosenbrock kernel");
+}
+
+template int launch_method_warp<KPP_PART>(LaunchArgs&, const double*, long, cudaStream_t);
+
 #else  // KPP_PART == 0
 
 thread_local char g_last_error[512] = "";
+
+// Rate constants that are fixed for a whole call (those depending only on
+// TEMP/CFACTOR, and the SUN-dependent ones when SUN is given per cell), one
+// thread per cell, into rates [NREACT][rates_ld]: the input of the warp
+// kernel, which keeps them in shared memory.
+__global__ void __launch_bounds__(128) rates_kernel(const LaunchArgs a, double* rates,
+                                                    long rates_ld) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= a.ncells) return;
+  CellEnv env;
+  load_env(env, a.temp, a.cfactor, a.sun, a.fix, a.ld, cell);
+  struct Col {
+    double* p;
+    long s;
+    __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * s]; }
+  } r{rates + cell, rates_ld}, v{a.var + cell, a.ld};
+  kpp_rconst_static(r, a.tstart[cell], env.temp, env.cfactor, 0.0, v, env.fix);
+  if (env.sun_fixed >= 0.0)
+    kpp_rconst_sun(r, a.tstart[cell], env.temp, env.cfactor, env.sun_fixed, v, env.fix);
+}
+
+size_t warp_smem_bytes() {
+  return sizeof(double) * (size_t)(6 * NVAR + 6 * NVAR + LU_NZ + NREACT +
+                                   (NREACT > kpp_warp::NB ? NREACT : kpp_warp::NB) + NFIX + 1);
+}
+
+// Which kernel integrates: 0 automatic (warp-cooperative for mechanisms with
+// a scratch work set that fits shared memory, else thread per cell), 1 thread
+// per cell, 2 warp per cell.
+int g_kernel_choice = 0;
+
+bool use_warp_kernel() {
+#if defined(KPP_SCRATCH)
+  // Auto picks the thread-per-cell kernel: on saprc99 (fresh cells) it
+  // measured 1.45x faster than the warp kernel, whose time goes to the
+  // sequential pivot / solve phases.
+  if (g_kernel_choice != 2) return false;
+  return warp_smem_bytes() <= 200 * 1024;
+#else
+  return false;
+#endif
+}
 
 // Per-cell evaluation of the mechanism functions (test and tooling entry).
 struct EvalArgs {
@@ -729,7 +802,45 @@ int cached_scratch(cudaStream_t stream, size_t bytes, double** out) {
   return KPP_B200_OK;
 }
 
+size_t scratch_capacity_doubles(const LaunchArgs& a) { return a.scratch_doubles; }
+
+int launch_warp(LaunchArgs& a, cudaStream_t s) {
+  // The rate pre-pass writes into the work buffer (which the warp kernel does
+  // not otherwise need), in chunks of cells that fit it.
+  const long cap = (long)(scratch_capacity_doubles(a) / NREACT);
+  if (cap < 1) return fail(KPP_B200_EINVAL, "work buffer too small for the rate constants");
+  for (long c0 = 0; c0 < a.ncells; c0 += cap) {
+    LaunchArgs b = a;
+    const long n = (a.ncells - c0 < cap) ? a.ncells - c0 : cap;
+    b.ncells = (int)n;
+    b.var = a.var + c0;
+    b.fix = a.fix ? a.fix + c0 : nullptr;
+    b.temp = a.temp + c0;
+    b.cfactor = a.cfactor ? a.cfactor + c0 : nullptr;
+    b.sun = a.sun ? a.sun + c0 : nullptr;
+    b.tstart = a.tstart + c0;
+    b.tend = a.tend + c0;
+    b.hstart = a.hstart ? a.hstart + c0 : nullptr;
+    b.istatus = a.istatus + c0;
+    b.rstatus = a.rstatus + c0;
+    b.ierr = a.ierr + c0;
+    rates_kernel<<<(int)((n + kBlock - 1) / kBlock), kBlock, 0, s>>>(b, a.scratch, n);
+    int rc = check_launch("rates_kernel");
+    if (rc != KPP_B200_OK) return rc;
+    switch (b.ipar[3]) {
+      case 1: rc = launch_method_warp<1>(b, a.scratch, n, s); break;
+      case 2: rc = launch_method_warp<2>(b, a.scratch, n, s); break;
+      case 3: rc = launch_method_warp<3>(b, a.scratch, n, s); break;
+      case 5: rc = launch_method_warp<5>(b, a.scratch, n, s); break;
+      default: rc = launch_method_warp<4>(b, a.scratch, n, s); break;
+    }
+    if (rc != KPP_B200_OK) return rc;
+  }
+  return KPP_B200_OK;
+}
+
 int launch_rosenbrock(LaunchArgs& a, cudaStream_t s) {
+  if (use_warp_kernel() && a.scratch) return launch_warp(a, s);
   const int grid = (int)(a.nslots / kBlock);
   // Invalid methods are reported per cell by the validation in
   // rosenbrock_cell (IERR = -2); any valid instance does that.
@@ -767,6 +878,7 @@ int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
   a.rstatus = rstatus;
   a.ierr = ierr;
   a.scratch = nullptr;
+  a.scratch_doubles = 0;
   a.nslots = 0;
   if (ipar) std::memcpy(a.ipar, ipar, sizeof a.ipar);
   if (rpar) std::memcpy(a.rpar, rpar, sizeof a.rpar);
@@ -919,6 +1031,7 @@ int host_pipeline(int ncells, int ld, double* var, const double* fix, const doub
     a.nslots = slots_for((int)n);
     int rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
     if (rc != KPP_B200_OK) return rc;
+    a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
     rc = launch_rosenbrock(a, s);
     if (rc != KPP_B200_OK) return rc;
 
@@ -994,6 +1107,7 @@ int kpp_b200_rosenbrock(int ncells, int ld, double* var, const double* fix, cons
   a.nslots = slots_for(ncells);
   rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
   if (rc != KPP_B200_OK) return rc;
+  a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
   return launch_rosenbrock(a, s);
 }
 
@@ -1016,6 +1130,7 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double* var, const double* fix, c
     if (!workspace || workspace_bytes < scratch_bytes(a.nslots))
       return fail(KPP_B200_EINVAL, "workspace smaller than kpp_b200_workspace_bytes()");
     a.scratch = (double*)workspace;
+    a.scratch_doubles = workspace_bytes / sizeof(double);
   }
   return launch_rosenbrock(a, (cudaStream_t)stream);
 }
@@ -1040,6 +1155,7 @@ int kpp_b200_rosenbrock_static(int ncells, int ld, double* var, const double* fi
   a.nslots = ((long)ncells + kBlock - 1) / kBlock * kBlock;
   rc = static_scratch(&a.scratch);
   if (rc != KPP_B200_OK) return rc;
+  a.scratch_doubles = a.scratch ? (size_t)kScratchPerSlot * kStaticMaxCells : 0;
   return launch_rosenbrock(a, (cudaStream_t)stream);
 }
 
@@ -1082,6 +1198,14 @@ int kpp_b200_decomp_solve(int ncells, int ld, double* jvs, double* x, int* ising
 }
 
 const char* kpp_b200_last_error(void) { return g_last_error; }
+
+int kpp_b200_set_kernel(int which) {
+  if (which < 0 || which > 2) return fail(KPP_B200_EINVAL, "kernel choice must be 0, 1 or 2");
+  g_kernel_choice = which;
+  return KPP_B200_OK;
+}
+
+int kpp_b200_get_kernel(void) { return use_warp_kernel() ? 2 : 1; }
 
 }  // extern "C"
 

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <memory>
@@ -237,6 +238,230 @@ int classify_rate(const std::string& e) {
     i++;
   }
   return cls;
+}
+
+
+// The double value C gives to the constant kppcu prints for float v.
+double const_value(float v) { return std::strtod(fmt_g(v).c_str(), nullptr); }
+
+// Head of a product tree built by mul(rate, stoich) in the reference's
+// folding: returns (rate index or -1, k1, k2) with value = (rate index >= 0 ?
+// RCT[idx] : k1) * (k2 unless k2 == 1).  Multiplying by an exact 1.0 changes
+// nothing, so applying k2 = 1 would also be exact; it is skipped.
+struct Head {
+  int rct;
+  double k1, k2;
+};
+
+Head head_of(const Mechanism& m, int eq, float stoich /* 1 for Fun */) {
+  const Reaction& r = m.reactions[eq];
+  Head h{-1, 1.0, 1.0};
+  if (r.kind != RATE_NUMBER) {
+    h.rct = eq;
+    h.k2 = (stoich == 1.0f) ? 1.0 : const_value(stoich);
+    return h;
+  }
+  float c = r.number;
+  if (stoich == 1.0f) { h.k1 = const_value(c); return h; }
+  if (c == 1.0f) { h.k1 = const_value(stoich); return h; }
+  h.k1 = const_value(c);
+  h.k2 = const_value(stoich);
+  return h;
+}
+
+template <class T>
+void emit_table(std::ostream& o, const char* type, const char* name, const std::vector<T>& v) {
+  o << "__device__ const " << type << " " << name << "[" << (v.empty() ? 1 : v.size()) << "] = {";
+  for (size_t i = 0; i < v.size(); i++) o << (i % 12 == 0 ? "\n    " : " ") << v[i] << ",";
+  if (v.empty()) o << "0";
+  o << "};\n";
+}
+
+void emit_dtable(std::ostream& o, const char* name, const std::vector<double>& v) {
+  o << "__device__ const double " << name << "[" << (v.empty() ? 1 : v.size()) << "] = {";
+  for (size_t i = 0; i < v.size(); i++) {
+    char buf[40];
+    std::snprintf(buf, sizeof buf, "%.17g", v[i]);
+    o << (i % 6 == 0 ? "\n    " : " ") << buf << ",";
+  }
+  if (v.empty()) o << "0";
+  o << "};\n";
+}
+
+// Schedules and operand tables of the warp-cooperative kernel, in which one
+// warp integrates one cell held in shared memory.  Every value is computed by
+// exactly the operation sequence of the unrolled functions above; only
+// independent computations run in parallel:
+//   Fun   A[j] products in parallel, then each Vdot row summed by one lane
+//   Jac   B products in parallel, then each JVS entry summed by one lane
+//   LU    right-looking by pivot: each element still gets its updates in
+//         increasing pivot order, the order of util/sutil.c's row loop
+//   solve forward by pivot (each row's terms in increasing column order);
+//         backward by dependency level, each row summed by one lane
+// Operand index convention for products: 0..NVAR-1 = V, NVAR.. = FIX, and
+// KPP_WOPND_ONE = the constant 1.0 (padding: x*1.0 == x exactly).
+void emit_warp_tables(std::ostream& o, const Mechanism& m) {
+  View vw(m);
+  const int nvar = m.nvar, nr = m.nreact();
+  const int ONE = m.nvar + m.nfix;
+  auto factors = [&](int eq, int skip, std::vector<int>& out) {
+    for (int i = 0; i < nvar; i++) {
+      int k = (int)vw.left(i, eq) - (i == skip ? 1 : 0);
+      for (int c = 0; c < k; c++) out.push_back(i);
+    }
+    for (int i = nvar; i < m.nspec; i++)
+      for (int c = 0; c < (int)vw.left(i, eq); c++) out.push_back(i);
+  };
+  int maxf = 1;
+  // --- Fun products
+  std::vector<int> a_eq, a_rct, a_f;
+  std::vector<double> a_k1, a_k2;
+  std::vector<std::vector<int>> a_fs;
+  for (int j = 0; j < nr; j++) {
+    bool used = false;
+    for (int i = 0; i < nvar; i++)
+      if (vw.net(i, j) != 0) { used = true; break; }
+    if (!used) continue;
+    Head h = head_of(m, j, 1.0f);
+    std::vector<int> f;
+    factors(j, -1, f);
+    maxf = std::max(maxf, (int)f.size());
+    a_eq.push_back(j); a_rct.push_back(h.rct); a_k1.push_back(h.k1); a_k2.push_back(h.k2);
+    a_fs.push_back(f);
+  }
+  // --- Jac products
+  std::vector<int> b_rct;
+  std::vector<double> b_k1, b_k2;
+  std::vector<std::vector<int>> b_fs;
+  std::vector<std::vector<int>> bidx(nr, std::vector<int>(nvar, -1));
+  for (int i = 0; i < nr; i++)
+    for (int j = 0; j < nvar; j++) {
+      if (vw.left(j, i) == 0) continue;
+      bidx[i][j] = (int)b_rct.size();
+      Head h = head_of(m, i, vw.left(j, i));
+      std::vector<int> f;
+      factors(i, j, f);
+      maxf = std::max(maxf, (int)f.size());
+      b_rct.push_back(h.rct); b_k1.push_back(h.k1); b_k2.push_back(h.k2); b_fs.push_back(f);
+    }
+  auto flat = [&](const std::vector<std::vector<int>>& fs) {
+    std::vector<int> out;
+    for (auto& f : fs)
+      for (int k = 0; k < maxf; k++) out.push_back(k < (int)f.size() ? f[k] : ONE);
+    return out;
+  };
+  // --- Vdot rows (CSR over species; terms in reaction order)
+  std::vector<int> v_ptr{0}, v_j;
+  std::vector<double> v_c;
+  for (int i = 0; i < nvar; i++) {
+    for (int j = 0; j < nr; j++) {
+      float c = vw.net(i, j);
+      if (c == 0) continue;
+      v_j.push_back(j);
+      v_c.push_back(const_value(c));
+    }
+    v_ptr.push_back((int)v_j.size());
+  }
+  // --- JVS entries (CSR over LU positions; terms in reaction order)
+  std::vector<int> j_ptr{0}, j_b;
+  std::vector<double> j_c;
+  for (int i = 0; i < nvar; i++)
+    for (int j = 0; j < nvar; j++) {
+      if (!(m.lustruct[i][j] || i == j)) continue;
+      if (m.lustruct[i][j])
+        for (int k = 0; k < nr; k++)
+          if (vw.net(i, k) * (bidx[k][j] >= 0 ? 1.0f : 0.0f) != 0) {
+            j_b.push_back(bidx[k][j]);
+            j_c.push_back(const_value(vw.net(i, k)));
+          }
+      j_ptr.push_back((int)j_b.size());
+    }
+  // --- LU by pivot
+  std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
+  for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
+  std::vector<int> lu_piv, lu_lptr{0}, lu_l, lu_uptr{0}, lu_ut, lu_um, lu_us;
+  for (int j = 0; j < nvar; j++) {
+    std::vector<int> rows;
+    for (int k = j + 1; k < nvar; k++)
+      if (pos[k][j] >= 0) rows.push_back(k);
+    if (rows.empty()) continue;
+    lu_piv.push_back(j);
+    for (int k : rows) lu_l.push_back(pos[k][j]);
+    lu_lptr.push_back((int)lu_l.size());
+    for (int k : rows)
+      for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
+        lu_ut.push_back(pos[k][m.lu_icol[jj]]);
+        lu_um.push_back(pos[k][j]);
+        lu_us.push_back(jj);
+      }
+    lu_uptr.push_back((int)lu_ut.size());
+  }
+  // --- forward solve by pivot
+  std::vector<int> fw_piv, fw_ptr{0}, fw_row, fw_pos;
+  for (int j = 0; j < nvar; j++) {
+    std::vector<int> rows;
+    for (int i = j + 1; i < nvar; i++)
+      if (pos[i][j] >= 0) rows.push_back(i);
+    if (rows.empty()) continue;
+    fw_piv.push_back(j);
+    for (int i : rows) { fw_row.push_back(i); fw_pos.push_back(pos[i][j]); }
+    fw_ptr.push_back((int)fw_row.size());
+  }
+  // --- backward solve by level: level(i) = 1 + max level(c), c > i in row i
+  std::vector<int> level(nvar, 0);
+  int nlev = 0;
+  for (int i = nvar - 1; i >= 0; i--) {
+    int lv = 0;
+    for (int jj = m.lu_diag[i] + 1; jj < m.lu_crow[i + 1]; jj++)
+      lv = std::max(lv, level[m.lu_icol[jj]] + 1);
+    level[i] = lv;
+    nlev = std::max(nlev, lv + 1);
+  }
+  std::vector<int> bw_lptr{0}, bw_rows;
+  for (int lv = 0; lv < nlev; lv++) {
+    for (int i = nvar - 1; i >= 0; i--)
+      if (level[i] == lv) bw_rows.push_back(i);
+    bw_lptr.push_back((int)bw_rows.size());
+  }
+
+  o << "\n// ---- schedules of the warp-cooperative kernel (one warp per cell) ----\n";
+  o << "namespace kpp_warp {\n";
+  o << "constexpr int KPP_WOPND_ONE = " << ONE << ";\n";
+  o << "constexpr int MAXF = " << maxf << ";\n";
+  o << "constexpr int NA = " << a_eq.size() << ", NB = " << b_rct.size()
+    << ", NPIV = " << lu_piv.size() << ", NFWP = " << fw_piv.size() << ", NLEV = " << nlev << ";\n";
+  emit_table(o, "int", "a_eq", a_eq);
+  emit_table(o, "int", "a_rct", a_rct);
+  emit_dtable(o, "a_k1", a_k1);
+  emit_dtable(o, "a_k2", a_k2);
+  emit_table(o, "short", "a_f", flat(a_fs));
+  emit_table(o, "int", "b_rct", b_rct);
+  emit_dtable(o, "b_k1", b_k1);
+  emit_dtable(o, "b_k2", b_k2);
+  emit_table(o, "short", "b_f", flat(b_fs));
+  emit_table(o, "int", "v_ptr", v_ptr);
+  emit_table(o, "short", "v_j", v_j);
+  emit_dtable(o, "v_c", v_c);
+  emit_table(o, "int", "j_ptr", j_ptr);
+  emit_table(o, "short", "j_b", j_b);
+  emit_dtable(o, "j_c", j_c);
+  emit_table(o, "int", "lu_diag", std::vector<int>(m.lu_diag.begin(), m.lu_diag.end() - 1));
+  emit_table(o, "int", "lu_piv", lu_piv);
+  emit_table(o, "int", "lu_lptr", lu_lptr);
+  emit_table(o, "short", "lu_l", lu_l);
+  emit_table(o, "int", "lu_uptr", lu_uptr);
+  emit_table(o, "short", "lu_ut", lu_ut);
+  emit_table(o, "short", "lu_um", lu_um);
+  emit_table(o, "short", "lu_us", lu_us);
+  emit_table(o, "int", "fw_piv", fw_piv);
+  emit_table(o, "int", "fw_ptr", fw_ptr);
+  emit_table(o, "short", "fw_row", fw_row);
+  emit_table(o, "short", "fw_pos", fw_pos);
+  emit_table(o, "int", "bw_lptr", bw_lptr);
+  emit_table(o, "short", "bw_rows", bw_rows);
+  emit_table(o, "int", "lu_crow", m.lu_crow);
+  emit_table(o, "short", "lu_icol", m.lu_icol);
+  o << "}  // namespace kpp_warp\n";
 }
 
 }  // namespace
@@ -490,6 +715,8 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     << "#define KPP_OPS_JAC " << ops_jac << "\n"
     << "#define KPP_OPS_DECOMP " << ops_decomp << "\n"
     << "#define KPP_OPS_SOLVE " << ops_solve << "\n";
+
+  emit_warp_tables(o, m);
 
   std::ofstream f(out_prefix + ".cuh");
   if (!f) return false;

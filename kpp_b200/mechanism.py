@@ -92,6 +92,7 @@ class Mechanism:
         L.kpp_b200_rosenbrock_host.argtypes = ros + [ctypes.c_int]
         L.kpp_b200_fun_jac.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 4
         L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
+        L.kpp_b200_set_kernel.argtypes = [ctypes.c_int]
 
     def _check(self, rc: int):
         if rc != KPP_B200_OK:
@@ -114,6 +115,14 @@ class Mechanism:
 
     def index(self, species: str) -> int:
         return self.species.index(species)
+
+    def set_kernel(self, which: str):
+        """'auto', 'thread' (one thread per cell) or 'warp' (one warp per cell,
+        work set in shared memory); both give bit-identical results."""
+        self._check(self.lib.kpp_b200_set_kernel({"auto": 0, "thread": 1, "warp": 2}[which]))
+
+    def kernel(self) -> str:
+        return {1: "thread", 2: "warp"}[self.lib.kpp_b200_get_kernel()]
 
     def workspace_bytes(self, ncells: int) -> int:
         return int(self.lib.kpp_b200_workspace_bytes(ncells))

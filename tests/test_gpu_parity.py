@@ -238,3 +238,31 @@ def test_host_entry_matches_device_entry():
     np.testing.assert_array_equal(rh.istatus.numpy(), r.istatus.cpu().numpy())
     np.testing.assert_array_equal(rh.rstatus.numpy(), r.rstatus.cpu().numpy())
     np.testing.assert_array_equal(rh.ierr.numpy(), r.ierr.cpu().numpy())
+
+
+@pytest.mark.parametrize("method", ["ros2", "ros3", "ros4", "rodas3", "rodas4"])
+@pytest.mark.parametrize("sun_mode", ["per_cell", "update_sun"])
+def test_warp_kernel_bit_identical_to_thread_kernel(method, sun_mode):
+    """The warp-per-cell kernel (work set in shared memory) and the
+    thread-per-cell kernel give the same bits: same operations, same order."""
+    m = load("saprc99")
+    wl = workloads.for_mechanism(m, "saprc99", 300, seed=41)
+    ipar, rpar = make_controls(method=method, scalar_tol=True)
+    t0, t1 = wl.step_bounds(0)
+    sun = dev(wl.sun) if sun_mode == "per_cell" else None
+    outs = []
+    try:
+        for which in ("thread", "warp"):
+            m.set_kernel(which)
+            assert m.kernel() == which
+            var = dev(wl.var)
+            r = m.rosenbrock(var, dev(wl.fix), dev(wl.temp), dev(t0), dev(t1), dev(wl.atol),
+                             dev(wl.rtol), ipar, rpar, cfactor=dev(wl.cfactor), sun=sun,
+                             hstart=dev(np.full(300, 10.0)))
+            torch.cuda.synchronize()
+            outs.append([var.cpu().numpy(), r.istatus.cpu().numpy(), r.rstatus.cpu().numpy(),
+                         r.ierr.cpu().numpy()])
+    finally:
+        m.set_kernel("auto")
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
