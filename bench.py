@@ -47,7 +47,7 @@ import numpy as np
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
-METRIC = "saprc99 cell-steps/s at 2^20 cells, learned-scheduled vs plain"
+METRIC = "saprc99 cell-steps/s at 2^20 cells, learned-scheduled vs plain, same accuracy"
 UNIT = "cell-steps/s"
 
 
@@ -181,7 +181,50 @@ def method_vector_ops(nvar: int, method: str, fixed_rates: bool) -> dict:
     return {"per_attempt": per_attempt, "per_step": per_step}
 
 
-def run_cuda_arm(args, rank, world, local_rank):
+def _tight_worker(args):
+    mech, var, fix, temp, cf, sun, t0, t1, ipar, rpar = args
+    sys.path.insert(0, str(REPO / "tests"))
+    from oracle_lib import OracleLib
+    o = OracleLib(mech)
+    v, _, _, ierr = o.integrate(var, fix, temp, t0, t1, np.array([TIGHT_ATOL]),
+                                np.array([TIGHT_RTOL]), ipar, rpar, cfactor=cf, sun=sun,
+                                which="or")
+    return v, ierr
+
+
+TIGHT_RTOL, TIGHT_ATOL = 1e-10, 1e-8
+
+
+def tight_reference(wl, cells, pool):
+    """FP64 Rodas4 solution at RTOL 1e-10 (ATOL 1e-8 molec/cm3) of the given
+    cells from their initial state over the first chemistry step, by the CPU
+    restatement of the reference Rosenbrock (oracle/ros_oracle.c)."""
+    from kpp_b200.controls import make_controls
+    ipar, rpar = make_controls(method="rodas4", scalar_tol=True)
+    t0, t1 = wl.step_bounds(0)
+    parts = np.array_split(cells, min(len(cells), os.cpu_count() or 1))
+    opt = lambda x, c: None if x is None else np.ascontiguousarray(x[c])
+    jobs = [(wl.mech, np.ascontiguousarray(wl.var[:, c]), np.ascontiguousarray(wl.fix[:, c]),
+             wl.temp[c], opt(wl.cfactor, c), opt(wl.sun, c), t0[c], t1[c], ipar, rpar)
+            for c in parts if len(c)]
+    res = pool.map(_tight_worker, jobs)
+    return np.concatenate([r[0] for r in res], axis=1), np.concatenate([r[1] for r in res])
+
+
+def accuracy(got: np.ndarray, ref: np.ndarray, atol: float, rtol: float) -> dict:
+    """Error of an RTOL 1e-3 solution against the tight one: the largest
+    relative error over species above 1e3 ATOL (where the relative tolerance
+    governs the solve), and the largest per-cell error in the integrator's own
+    norm, sqrt(mean(((y - ref) / (ATOL + RTOL |ref|))^2))."""
+    mask = np.abs(ref) > 1e3 * atol
+    rel = np.abs(got - ref)[mask] / np.abs(ref)[mask]
+    norm = np.sqrt((((got - ref) / (atol + rtol * np.abs(ref))) ** 2).mean(axis=0))
+    return {"max_rel_err_above_1e3_atol": float(rel.max()) if rel.size else None,
+            "median_rel_err_above_1e3_atol": float(np.median(rel)) if rel.size else None,
+            "max_cell_error_norm": float(norm.max()), "cells": int(ref.shape[1])}
+
+
+def run_cuda_arm(args, rank, world, local_rank, pool=None):
     import torch
     from kpp_b200 import load, workloads
     from kpp_b200.build import LIB
@@ -201,63 +244,108 @@ def run_cuda_arm(args, rank, world, local_rank):
     atol, rtol = D(wl.atol), D(wl.rtol)
     total = args.warmup + args.steps
     t_bounds = [(D(wl.step_bounds(k)[0]), D(wl.step_bounds(k)[1])) for k in range(total)]
-    hstart = torch.zeros(n, dtype=torch.float64, device=dev)
-    out = None
     stream = torch.cuda.current_stream(dev)
-
     fresh = args.mode == "fresh"
-    var0 = var.clone() if fresh else None
+    var0 = var.clone()
 
-    def step(k):
-        nonlocal out, hstart
-        if fresh:
-            var.copy_(var0)  # the same fresh batch every step
-            out = mech.rosenbrock(var, fix, temp, t_bounds[0][0], t_bounds[0][1], atol, rtol,
-                                  wl.ipar, wl.rpar, cfactor=cf, sun=sun, out=out)
-            return
-        out = mech.rosenbrock(var, fix, temp, t_bounds[k][0], t_bounds[k][1], atol, rtol,
-                              wl.ipar, wl.rpar, cfactor=cf, sun=sun, hstart=hstart, out=out)
-        hstart = out.rstatus[1].clone()
+    sched, sched_note = None, None
+    if args.scheduler == "learned":
+        from kpp_b200.scheduler import LearnedScheduler
+        wpath = Path(args.weights) if args.weights else (
+            REPO / "kpp_b200" / "schedulers" / f"{args.workload}.npz")
+        if wpath.exists():
+            sched = LearnedScheduler.load(wpath, mech.nvar)
+        else:
+            sched_note = f"no trained scheduler at {wpath}: plain only"
 
     def barrier():
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
 
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-
-    # state at the start of the timed steps; the end-to-end run replays the
-    # same steps from it
-    snap_var = (var0 if fresh else var).cpu().numpy().copy()
-    snap_hs = hstart.cpu().numpy().copy()
-
-    # ---- device-timed region: inputs resident in HBM (larger than L2)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stats = []
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        ev0.record(stream)
-        for k in range(args.warmup, total):
-            step(k)
-            stats.append(out.istatus.sum(dim=1))  # device-side reduction, no sync
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    ierr = out.ierr.cpu().numpy()
-    ist_sum = torch.stack(stats).sum(dim=0).cpu().numpy().astype(np.int64)
-    ms_max = ms
-    if world > 1:
+    def max_over_ranks(ms):
+        if world == 1:
+            return ms
         import torch.distributed as dist
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * n * args.steps / (ms_max / 1e3)
+        return float(t.item())
 
-    # ---- algorithmic FP64 work of the timed steps (exact counts from ISTATUS)
+    class Arm:
+        """One way of running the steps: plain (grid-stride kernel, Hstart =
+        STEPMIN) or learned (plan, then the work-queue kernel in cost order
+        with the planned Hstart)."""
+
+        def __init__(self, learned):
+            self.learned = learned
+            self.out = None
+            self.hs = torch.zeros(n, dtype=torch.float64, device=dev)
+            self.hs_plan = torch.empty(n, dtype=torch.float64, device=dev)
+            self.order = torch.empty(n, dtype=torch.int32, device=dev)
+
+        def step(self, k):
+            kk = 0 if fresh else k
+            if fresh:
+                var.copy_(var0)  # the same fresh batch every step
+            t0, t1 = t_bounds[kk]
+            warm = None if fresh else self.hs
+            if not self.learned:
+                self.out = mech.rosenbrock(var, fix, temp, t0, t1, atol, rtol, wl.ipar, wl.rpar,
+                                           cfactor=cf, sun=sun, hstart=warm, out=self.out)
+            else:
+                sched.plan(var, temp, t0, cfactor=cf, sun=sun, tend=t1, hstart=self.hs_plan,
+                           order=self.order)
+                self.out = mech.rosenbrock_chain(
+                    var, fix, temp, t0, wl.dt, 1, atol, rtol, wl.ipar, wl.rpar, cfactor=cf,
+                    sun=sun, hstart=self.hs_plan if fresh else warm, order=self.order,
+                    out=self.out)
+            if not fresh:
+                self.hs = self.out.rstatus[1].clone()
+
+        def run(self):
+            """Warm-up steps, then the timed steps; returns ms and ISTATUS sums."""
+            var.copy_(var0)
+            self.hs.zero_()
+            for k in range(args.warmup):
+                self.step(k)
+            torch.cuda.synchronize()
+            self.snap_var = var.cpu().numpy() if not fresh else None
+            self.snap_hs = self.hs.cpu().numpy().copy()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            stats = []
+            barrier()
+            torch.cuda.synchronize()
+            with ClockSampler(local_rank) as clk:
+                ev0.record(stream)
+                for k in range(args.warmup, total):
+                    self.step(k)
+                    stats.append(self.out.istatus.sum(dim=1))  # device reduction, no sync
+                ev1.record(stream)
+                torch.cuda.synchronize()
+            barrier()
+            self.ms = max_over_ranks(ev0.elapsed_time(ev1))
+            self.clocks = clk.summary()
+            self.ierr = self.out.ierr.cpu().numpy()
+            self.var_out = var.cpu().numpy()
+            self.ist = torch.stack(stats).sum(dim=0).cpu().numpy().astype(np.int64)
+            self.value = world * n * args.steps / (self.ms / 1e3)
+            return self
+
+        def summary(self):
+            nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng = self.ist.tolist()
+            return {"value": self.value, "unit": UNIT, "ms_per_step": self.ms / args.steps,
+                    "internal_steps_per_cell_step": nstp / (n * args.steps),
+                    "rejected_step_rate": nrej / max(nstp, 1),
+                    "ierr_ok_fraction": float((self.ierr == 1).mean()),
+                    "clocks": self.clocks,
+                    "istatus_sum": dict(zip(["nfun", "njac", "nstp", "nacc", "nrej", "ndec",
+                                             "nsol", "nsng"], map(int, self.ist)))}
+
+    plain = Arm(False).run()
+    learned = Arm(True).run() if sched is not None else None
+    head = learned if learned is not None else plain
+
+    # ---- algorithmic FP64 work of the headline arm's timed steps (ISTATUS counts)
     hdr = (REPO / "kpp_b200" / "_gen" / f"{args.mech}.cuh")
     opsd = {}
     if hdr.exists():
@@ -265,46 +353,93 @@ def run_cuda_arm(args, rank, world, local_rank):
             if line.startswith("#define KPP_OPS_"):
                 _, k, v = line.split()
                 opsd[k[8:].lower()] = int(v)
-    nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng = ist_sum.tolist()
+    nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng = head.ist.tolist()
     fixed_rates = sun is not None
     vec = method_vector_ops(mech.nvar, "rodas3", fixed_rates)
     fun_evals = nfun - (njac if fixed_rates else 0)   # dF/dT Fun elided for fixed rates
     flops = (fun_evals * opsd.get("fun", 0) + ndec * (opsd.get("jac", 0) + opsd.get("decomp", 0))
              + nsol * opsd.get("solve", 0) + nstp * vec["per_attempt"] + njac * vec["per_step"])
-    achieved_tflops = flops / (ms / 1e3) / 1e12
+    achieved_tflops = flops / (head.ms / 1e3) / 1e12
     peak_fma, peak_muladd = fp64_peak(LIB / "libkpp_b200_util.so")
 
-    # ---- end to end through the public API with host buffers: the same timed
-    # steps, from the same state, through kpp_b200_rosenbrock_host (pinned host
-    # arrays in, results back in host memory every step)
+    # ---- end to end through the public API with host buffers (pinned host
+    # arrays in, every output back in host memory, each step)
     e2e = None
     if args.e2e:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-        h_var, h_fix, h_temp = pin(snap_var), pin(wl.fix), pin(wl.temp)
+        h_var0 = pin(wl.var if fresh else head.snap_var)
+        h_var = h_var0.clone()
+        h_fix, h_temp = pin(wl.fix), pin(wl.temp)
         h_cf = pin(wl.cfactor) if wl.cfactor is not None else None
         h_sun = pin(wl.sun) if wl.sun is not None else None
         h_atol, h_rtol = pin(wl.atol), pin(wl.rtol)
         h_t = [(pin(wl.step_bounds(k)[0]), pin(wl.step_bounds(k)[1])) for k in range(total)]
-        h_hs = pin(snap_hs)
-        res = None
+        h_hs = pin(head.snap_hs)
+        nb = lambda x: 0 if x is None else x.numel() * x.element_size()
+        if learned is not None:
+            # the learned scheduler through its Python API: copy in, plan,
+            # integrate in cost order, copy out
+            d_in = {}
+            res = {"ist": torch.empty(8, n, dtype=torch.int32).pin_memory(),
+                   "rst": torch.empty(2, n, dtype=torch.float64).pin_memory(),
+                   "ierr": torch.empty(n, dtype=torch.int32).pin_memory()}
+            hs_d = torch.empty(n, dtype=torch.float64, device=dev)
+            order_d = torch.empty(n, dtype=torch.int32, device=dev)
+            out_box = [None]
 
-        h_var0 = h_var.clone() if fresh else None
+            def e2e_step(k):
+                kk = 0 if fresh else k
+                if fresh:
+                    h_var.copy_(h_var0)
+                for nm, h in (("var", h_var), ("fix", h_fix), ("temp", h_temp), ("cf", h_cf),
+                              ("sun", h_sun), ("atol", h_atol), ("rtol", h_rtol),
+                              ("t0", h_t[kk][0]), ("t1", h_t[kk][1]),
+                              ("hs", None if fresh else h_hs)):
+                    if h is not None:
+                        if nm not in d_in:
+                            d_in[nm] = torch.empty_like(h, device=dev)
+                        d_in[nm].copy_(h, non_blocking=True)
+                sched.plan(d_in["var"], d_in["temp"], d_in["t0"], cfactor=d_in.get("cf"),
+                           sun=d_in.get("sun"), tend=d_in["t1"], hstart=hs_d, order=order_d)
+                out_box[0] = o = mech.rosenbrock_chain(
+                    d_in["var"], d_in["fix"], d_in["temp"], d_in["t0"], wl.dt, 1, d_in["atol"],
+                    d_in["rtol"], wl.ipar, wl.rpar, cfactor=d_in.get("cf"), sun=d_in.get("sun"),
+                    hstart=hs_d if fresh else d_in["hs"], order=order_d, out=out_box[0])
+                h_var.copy_(d_in["var"], non_blocking=True)
+                res["ist"].copy_(o.istatus, non_blocking=True)
+                res["rst"].copy_(o.rstatus, non_blocking=True)
+                res["ierr"].copy_(o.ierr, non_blocking=True)
+                torch.cuda.current_stream(dev).synchronize()
+                if not fresh:
+                    h_hs.copy_(res["rst"][1])
 
-        def e2e_step(k):
-            nonlocal res
-            if fresh:
-                h_var.copy_(h_var0)  # the host model hands in the same fresh cells
-                res = mech.rosenbrock_host(h_var, h_fix, h_temp, h_t[0][0], h_t[0][1], h_atol,
-                                           h_rtol, wl.ipar, wl.rpar, cfactor=h_cf, sun=h_sun,
-                                           out=res)
-                return
-            res = mech.rosenbrock_host(h_var, h_fix, h_temp, h_t[k][0], h_t[k][1], h_atol, h_rtol,
-                                       wl.ipar, wl.rpar, cfactor=h_cf, sun=h_sun, hstart=h_hs,
-                                       out=res)
-            h_hs.copy_(res.rstatus[1])  # the host model's warm start for its next call
+            h2d = sum(nb(x) for x in (h_var, h_fix, h_temp, h_cf, h_sun, h_atol, h_rtol,
+                                      h_t[0][0], h_t[0][1], None if fresh else h_hs))
+            d2h = nb(h_var) + nb(res["ist"]) + nb(res["rst"]) + nb(res["ierr"])
+            api = ("kpp_b200.scheduler.LearnedScheduler.plan + Mechanism.rosenbrock_chain "
+                   "(kpp_sched_plan + kpp_b200_rosenbrock_chain), pinned host arrays copied in "
+                   "and out every step")
+        else:
+            res_box = [None]
 
+            def e2e_step(k):
+                kk = 0 if fresh else k
+                if fresh:
+                    h_var.copy_(h_var0)  # the host model hands in the same fresh cells
+                res_box[0] = mech.rosenbrock_host(
+                    h_var, h_fix, h_temp, h_t[kk][0], h_t[kk][1], h_atol, h_rtol, wl.ipar,
+                    wl.rpar, cfactor=h_cf, sun=h_sun, hstart=None if fresh else h_hs,
+                    out=res_box[0])
+                if not fresh:
+                    h_hs.copy_(res_box[0].rstatus[1])  # the host model's warm start
+
+            h2d = sum(nb(x) for x in (h_var, h_fix, h_temp, h_cf, h_sun, h_t[0][0], h_t[0][1],
+                                      None if fresh else h_hs))
+            d2h = nb(h_var) + 8 * n * 4 + 2 * n * 8 + n * 4
+            api = ("kpp_b200_rosenbrock_host (pinned host arrays, chunked copies overlapped "
+                   "with the integration, synchronous)")
         keep_var, keep_hs = h_var.clone(), h_hs.clone()
-        e2e_step(args.warmup)  # warm the pipeline, then replay the timed steps
+        e2e_step(args.warmup)  # warm the path, then replay the timed steps
         h_var.copy_(keep_var)
         h_hs.copy_(keep_hs)
         torch.cuda.synchronize()
@@ -312,42 +447,65 @@ def run_cuda_arm(args, rank, world, local_rank):
         t_start = time.perf_counter()
         for k in range(args.warmup, total):
             e2e_step(k)
-        ems = (time.perf_counter() - t_start) * 1e3
+        ems = max_over_ranks((time.perf_counter() - t_start) * 1e3)
         barrier()
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ems], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        nb = lambda x: 0 if x is None else x.numel() * x.element_size()
-        h2d = sum(nb(x) for x in (h_var, h_fix, h_temp, h_cf, h_sun, h_t[0][0], h_t[0][1],
-                                  None if fresh else h_hs))
-        d2h = nb(h_var) + nb(res.istatus) + nb(res.rstatus) + nb(res.ierr)
-        same = bool(np.array_equal(h_var.numpy(), var.cpu().numpy()))
+        same = bool(np.array_equal(h_var.numpy(), head.var_out))
         e2e = {"value": world * n * args.steps / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": ems / args.steps, "api": "kpp_b200_rosenbrock_host (pinned host "
-               "arrays, chunked copies overlapped with the integration, synchronous)",
-               "matches_device_run": same}
+               "ms_per_step": ems / args.steps, "api": api, "matches_device_run": same}
 
+    sched_block = {"kind": "learned" if learned is not None else "plain"}
+    if learned is not None:
+        # the plan alone (features, network, binning) on the fresh batch
+        var.copy_(var0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            sched.plan(var, temp, t_bounds[0][0], cfactor=cf, sun=sun, tend=t_bounds[0][1])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sched_block.update({
+            "speedup_vs_plain": learned.value / plain.value,
+            "plan_ms": e0.elapsed_time(e1) / 3,
+            "ierr_identical_to_plain": bool(np.array_equal(learned.ierr, plain.ierr)),
+            "network": "78 features -> 3 x 256 GELU -> 2 (log10 Hstart, ln Nstp); BF16 "
+                       "mma.sync GEMMs, FP32 accumulate; trained on the GPU by "
+                       "kpp_b200.train_scheduler",
+            "weights": sched.meta.get("source"),
+        })
+    elif sched_note:
+        sched_block["note"] = sched_note
+    if pool is not None and fresh and args.accuracy_cells > 0:
+        cells = np.linspace(0, n - 1, args.accuracy_cells).astype(np.int64)
+        ref, ref_ierr = tight_reference(wl, cells, pool)
+        acc = {"plain": accuracy(plain.var_out[:, cells], ref, float(wl.atol[0]),
+                                 float(wl.rtol[0])),
+               "oracle_ierr_ok": bool((ref_ierr == 1).all())}
+        if learned is not None:
+            acc["learned"] = accuracy(learned.var_out[:, cells], ref, float(wl.atol[0]),
+                                      float(wl.rtol[0]))
+        sched_block["accuracy_vs_fp64_rtol1e-10"] = acc
+
+    nchunks = (n + (1 << 17) - 1) >> 17
+    launches_learned = nchunks * (1 + 4) + 2 + 1
     result = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "metric": METRIC, "value": head.value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head.ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.mech} {args.workload} ({args.mode}) plain Rodas3, {n} cells "
+        "config": {"workload": f"{args.mech} {args.workload} ({args.mode}) Rodas3, {n} cells "
                                f"per GPU, 600 s chemistry step, RTOL 1e-3 ATOL 1e-2",
-                   "mode": args.mode,
-                   "cells_per_gpu": n, "chemistry_step_s": wl.dt, "method": "rodas3",
-                   "scheduler": "plain", "parallelism": f"cell shards x{world}",
+                   "mode": args.mode, "cells_per_gpu": n, "chemistry_step_s": wl.dt,
+                   "method": "rodas3", "scheduler": sched_block["kind"],
+                   "parallelism": f"cell shards x{world}",
                    "kernel": {"thread": "thread per cell", "warp": "warp per cell"}[kernel],
                    "l2": "inputs larger than L2 (VAR alone %d MB)" % (wl.var.nbytes >> 20)},
         "impl": "kpp_b200",
-        "gpu_launches": args.steps * (2 if kernel == "warp" else 1),
-        "stats": {"internal_steps_per_cell_step": nstp / (n * args.steps),
-                  "rejected_per_cell_step": nrej / (n * args.steps),
-                  "ierr_ok_fraction": float((ierr == 1).mean()),
-                  "istatus_sum": dict(zip(["nfun", "njac", "nstp", "nacc", "nrej", "ndec", "nsol",
-                                           "nsng"], map(int, ist_sum)))},
+        "gpu_launches": args.steps * (launches_learned if learned is not None
+                                      else (2 if kernel == "warp" else 1)),
+        "plain": plain.summary(),
+        "learned": learned.summary() if learned is not None else None,
+        "scheduler": sched_block,
+        "stats": head.summary(),
         "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": peak_fma,
                      "unit": "TFLOP/s", "frac": achieved_tflops / peak_fma if peak_fma > 0 else None,
                      "traffic": None,
@@ -355,7 +513,7 @@ def run_cuda_arm(args, rank, world, local_rank):
                                     "(kpp_b200/csrc/kpp_util.cu); MEASURED_PEAKS.json has no FP64 figure",
                      "peak_mul_add_tflops": peak_muladd,
                      "flops_per_cell_step": flops / (n * args.steps)},
-        "clocks": clk.summary(),
+        "clocks": head.clocks,
         "e2e": e2e,
     }
     return result, wl
@@ -375,6 +533,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--kernel", choices=["auto", "thread", "warp"], default="auto")
+    ap.add_argument("--scheduler", choices=["learned", "plain"], default="learned")
+    ap.add_argument("--weights", default=None, help="trained scheduler (.npz)")
+    ap.add_argument("--accuracy-cells", type=int, default=64)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -426,7 +587,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    result, wl = run_cuda_arm(args, rank, world, local_rank)
+    result, wl = run_cuda_arm(args, rank, world, local_rank, pool)
     if pool is not None:
         n_sample, _ = calibrated_sample(wl, procs, pool, target_s=args.cpu_seconds)
         rate, wall = cpu_reference_rate(wl, n_sample, procs, "", pool)

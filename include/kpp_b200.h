@@ -98,6 +98,34 @@ int kpp_b200_rosenbrock(int ncells, int ld, double *var, const double *fix,
                         int *istatus, double *rstatus, int *ierr,
                         void *stream);
 
+/* The host model's time loop (drv/general.c:59-76) over INTEGRATE
+ * (int/rosenbrock.c:94-133) for every cell in one persistent launch: each cell
+ * makes ncalls consecutive calls Rosenbrock(T, T + dt) with T = tstart[c]
+ * first and T += dt after each call; the first call's Hstart is hstart[c]
+ * (RPAR[2] when hstart is NULL), every later call's Hstart is the previous
+ * call's Hexit (INTEGRATE's STEPMIN = RPAR[11]).  A failing call does not
+ * stop the cell (the reference driver goes on after INTEGRATE reports it).
+ * Outputs: var after the last call; istatus[8][ld] summed over the calls
+ * (as INTEGRATE sums Ns/Na/Nr/Ng); rstatus[2][ld] Texit/Hexit of the last
+ * call; ierr[ld] the first failing call's IERR, 1 when all succeed.
+ * Equal, bit for bit, to ncalls kpp_b200_rosenbrock calls chained that way.
+ * Cells are handed to warps through a device work queue, 32 at a time, in
+ * the order order[0..ncells-1] (a permutation of 0..ncells-1; NULL for
+ * 0,1,...); per-cell results do not depend on the order, the run time does:
+ * the cost-binning scheduler passes cells sorted by decreasing predicted
+ * cost.  Device pointers, asynchronous; the first call per (device, stream)
+ * allocates the workspace and queue counter, so make it before capturing
+ * the stream into a CUDA graph.  Uses the thread-per-cell kernel. */
+int kpp_b200_rosenbrock_chain(int ncells, int ld, double *var,
+                              const double *fix, const double *temp,
+                              const double *cfactor, const double *sun,
+                              const double *tstart, double dt, int ncalls,
+                              const double *atol, const double *rtol,
+                              const int *ipar, const double *rpar,
+                              const double *hstart, const int *order,
+                              int *istatus, double *rstatus, int *ierr,
+                              void *stream);
+
 /* Device workspace (bytes) that kpp_b200_rosenbrock_ws uses at most for a
  * batch of ncells cells; 0 for mechanisms whose work arrays fit in registers.
  * No counterpart in the reference (its integrator keeps its work arrays on

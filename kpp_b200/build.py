@@ -174,6 +174,25 @@ def build_util(force: bool = False) -> Path:
     return lib
 
 
+def build_sched(force: bool = False) -> Path:
+    """libkpp_b200_sched.so: the learned scheduler (features, BF16 tensor-core
+    MLP, training kernels, scheduling pass); mechanism independent."""
+    LIB.mkdir(exist_ok=True)
+    BUILD.mkdir(exist_ok=True)
+    src = CSRC / "kpp_sched.cu"
+    deps = [src, CSRC / "kpp_ratelaws.cuh", INCLUDE / "kpp_sched.h"]
+    lib = LIB / "libkpp_b200_sched.so"
+    flags = ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-lineinfo",
+                    "-I", str(INCLUDE), "-I", str(CSRC)]
+    stamp = BUILD / "sched.stamp"
+    digest = _hash_files(deps, " ".join(flags))
+    if not force and lib.exists() and stamp.exists() and stamp.read_text() == digest:
+        return lib
+    _run([nvcc()] + flags + [str(src), "-o", str(lib)])
+    stamp.write_text(digest)
+    return lib
+
+
 def all_mechanisms():
     return sorted(p.stem for p in MECH_DIR.glob("*.kpp"))
 
@@ -182,7 +201,7 @@ def build(mechs=None, force: bool = False, jobs: int | None = None, verbose: boo
     kpp_home = default_kpp_home()
     jobs = jobs or os.cpu_count() or 4
     mechs = mechs or all_mechanisms()
-    built = {"util": build_util(force)}
+    built = {"util": build_util(force), "sched": build_sched(force)}
     for mech in mechs:
         header = generate(mech, kpp_home, force)
         if header is None:

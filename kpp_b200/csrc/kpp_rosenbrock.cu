@@ -194,6 +194,13 @@ struct LaunchArgs {
   size_t scratch_doubles;  // capacity of `scratch`
   int ipar[20];
   double rpar[20];
+  // Work queue and chained calls (kpp_b200_rosenbrock_chain); zero/null for
+  // the single-call entries.
+  const int* order;  // queue position -> cell, or null for the identity
+  int* queue;        // device counter of cells handed out (zero at launch), or
+                     // null for the grid-stride loop
+  int nchain;        // > 0: that many calls [T, T + chain_dt], T += chain_dt
+  double chain_dt;
 };
 
 struct Stats {
@@ -550,8 +557,58 @@ size_t warp_smem_bytes();
 #define KPP_MIN_BLOCKS 8
 #endif
 
-// One thread slot integrates cells slot, slot + nslots, ... (grid-stride).
-template <int METHOD>
+// Integrates one cell: one Rosenbrock call over [tstart, tend], or with
+// CHAIN (a.nchain >= 1) the driver loop of drv/general.c:59-76 around
+// INTEGRATE (int/rosenbrock.c:94-133): a.nchain calls Rosenbrock(T, T + dt),
+// T += dt, each call's Hstart = the previous call's Hexit (STEPMIN), counters
+// summed (INTEGRATE's Ns/Na/Nr/Ng), Texit/Hexit of the last call, IERR of the
+// first failing call (1 when every call succeeds).  Failing calls do not stop
+// the loop, as the reference driver continues after INTEGRATE reports them.
+template <int METHOD, bool CHAIN, class W>
+__device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, int cell) {
+  const long ld = a.ld;
+  CellEnv env;
+  load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
+#pragma unroll 4
+  for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
+
+  const int ncalls = CHAIN ? a.nchain : 1;
+  double t0 = a.tstart[cell];
+  double rpar2 = a.hstart ? a.hstart[cell] : a.rpar[2];
+  for (int k = 0; k < ncalls; k++) {
+    const double t1 = CHAIN ? t0 + a.chain_dt : a.tend[cell];
+    Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
+    double texit = 0.0, hexit = 0.0;
+    const int ierr = rosenbrock_cell<METHOD>(env, w, t0, t1, a.atol, a.rtol, a, rpar2, st,
+                                             texit, hexit);
+    // y is untouched when the controls were rejected (IERR -1..-5); the
+    // statistics and Texit/Hexit are then zero, as IPAR/RPAR[10..] stay.
+    const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
+    if (!CHAIN || k == 0) {
+      a.ierr[cell] = ierr;
+#pragma unroll
+      for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
+    } else {
+      if (a.ierr[cell] == KPP_B200_IERR_SUCCESS) a.ierr[cell] = ierr;
+#pragma unroll
+      for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] += sv[i];
+    }
+    a.rstatus[cell] = texit;
+    a.rstatus[ld + cell] = hexit;
+    rpar2 = hexit;  // STEPMIN = RPAR[11]
+    t0 = t1;        // TIME += DT
+  }
+#pragma unroll 4
+  for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+}
+
+// QUEUE = false: one thread slot integrates cells slot, slot + nslots, ...
+// (grid-stride), one call each.  QUEUE = true: each warp takes the next 32
+// queue positions from the device counter until the queue is empty
+// (persistent launch: the grid is the resident thread count) and runs the
+// chained calls of each cell.  A queue ordered by decreasing cost hands the
+// long cells out first and keeps the 32 cells of a warp of similar cost.
+template <int METHOD, bool QUEUE>
 __global__ void
 #if KPP_MIN_BLOCKS > 0
 __launch_bounds__(128, KPP_MIN_BLOCKS)
@@ -560,45 +617,38 @@ __launch_bounds__(128)
 #endif
 rosenbrock_kernel(const LaunchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long ld = a.ld;
   Work w(a.scratch, a.nslots, slot);
-  for (long c = slot; c < a.ncells; c += a.nslots) {
-    const int cell = (int)c;
-    CellEnv env;
-    load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
-#pragma unroll 4
-    for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
-
-    Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
-    double texit = 0.0, hexit = 0.0;
-    const double rpar2 = a.hstart ? a.hstart[cell] : a.rpar[2];
-    int ierr = rosenbrock_cell<METHOD>(env, w, a.tstart[cell], a.tend[cell], a.atol, a.rtol, a,
-                                       rpar2, st, texit, hexit);
-
-    // y is untouched when the controls were rejected (IERR -1..-5); the
-    // statistics and Texit/Hexit are then zero, as IPAR/RPAR[10..] stay.
-    a.ierr[cell] = ierr;
-#pragma unroll 4
-    for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
-    const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
-#pragma unroll
-    for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
-    a.rstatus[cell] = texit;
-    a.rstatus[ld + cell] = hexit;
+  if (QUEUE) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(a.queue, 32);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= a.ncells) break;  // warp-uniform
+      const int pos = base + lane;
+      if (pos < a.ncells) integrate_cell_calls<METHOD, true>(a, w, a.order ? a.order[pos] : pos);
+    }
+  } else {
+    for (long c = slot; c < a.ncells; c += a.nslots)
+      integrate_cell_calls<METHOD, false>(a, w, (int)c);
   }
 }
 
 
 template <int M>
 int launch_method(LaunchArgs& a, int grid, cudaStream_t s) {
-  rosenbrock_kernel<M><<<grid, kBlock, 0, s>>>(a);
+  if (a.queue)
+    rosenbrock_kernel<M, true><<<grid, kBlock, 0, s>>>(a);
+  else
+    rosenbrock_kernel<M, false><<<grid, kBlock, 0, s>>>(a);
   return check_launch("rosenbrock_kernel");
 }
 
 template <int M>
 int occupancy_method() {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rosenbrock_kernel<M>, kBlock, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rosenbrock_kernel<M, false>, kBlock,
+                                                    0) !=
       cudaSuccess)
     per_sm = 1;
   return per_sm;
@@ -802,6 +852,27 @@ int cached_scratch(cudaStream_t stream, size_t bytes, double** out) {
   return KPP_B200_OK;
 }
 
+// Work-queue counter, one per (device, stream), kept until exit.
+int cached_counter(cudaStream_t stream, int** out) {
+  static std::mutex mu;
+  static std::map<std::pair<int, cudaStream_t>, int*> cache;
+  *out = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  std::lock_guard<std::mutex> lock(mu);
+  int*& p = cache[{dev, stream}];
+  if (!p) {
+    e = cudaMalloc(&p, 256);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_fail("cudaMalloc(queue counter)", e);
+    }
+  }
+  *out = p;
+  return KPP_B200_OK;
+}
+
 size_t scratch_capacity_doubles(const LaunchArgs& a) { return a.scratch_doubles; }
 
 int launch_warp(LaunchArgs& a, cudaStream_t s) {
@@ -840,7 +911,7 @@ int launch_warp(LaunchArgs& a, cudaStream_t s) {
 }
 
 int launch_rosenbrock(LaunchArgs& a, cudaStream_t s) {
-  if (use_warp_kernel() && a.scratch) return launch_warp(a, s);
+  if (use_warp_kernel() && a.scratch && !a.queue && a.nchain == 0) return launch_warp(a, s);
   const int grid = (int)(a.nslots / kBlock);
   // Invalid methods are reported per cell by the validation in
   // rosenbrock_cell (IERR = -2); any valid instance does that.
@@ -880,6 +951,10 @@ int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
   a.scratch = nullptr;
   a.scratch_doubles = 0;
   a.nslots = 0;
+  a.order = nullptr;
+  a.queue = nullptr;
+  a.nchain = 0;
+  a.chain_dt = 0.0;
   if (ipar) std::memcpy(a.ipar, ipar, sizeof a.ipar);
   if (rpar) std::memcpy(a.rpar, rpar, sizeof a.rpar);
   return KPP_B200_OK;
@@ -1108,6 +1183,34 @@ int kpp_b200_rosenbrock(int ncells, int ld, double* var, const double* fix, cons
   rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
   if (rc != KPP_B200_OK) return rc;
   a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+  return launch_rosenbrock(a, s);
+}
+
+int kpp_b200_rosenbrock_chain(int ncells, int ld, double* var, const double* fix,
+                              const double* temp, const double* cfactor, const double* sun,
+                              const double* tstart, double dt, int ncalls, const double* atol,
+                              const double* rtol, const int* ipar, const double* rpar,
+                              const double* hstart, const int* order, int* istatus,
+                              double* rstatus, int* ierr, void* stream) {
+  LaunchArgs a;
+  // tend is not read in chained mode; tstart stands in for the null check
+  int rc = fill_args(a, ncells, ld, var, fix, temp, cfactor, sun, tstart, tstart, atol, rtol,
+                     ipar, rpar, hstart, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK) return rc;
+  if (ncalls < 1) return fail(KPP_B200_EINVAL, "ncalls must be >= 1");
+  if (ncells == 0) return KPP_B200_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  a.nchain = ncalls;
+  a.chain_dt = dt;
+  a.order = order;
+  a.nslots = slots_for(ncells);
+  rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+  if (rc != KPP_B200_OK) return rc;
+  a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+  rc = cached_counter(s, &a.queue);
+  if (rc != KPP_B200_OK) return rc;
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(int), s);
+  if (e != cudaSuccess) return cuda_fail("cudaMemsetAsync(queue counter)", e);
   return launch_rosenbrock(a, s);
 }
 

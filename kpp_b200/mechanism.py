@@ -93,6 +93,10 @@ class Mechanism:
         L.kpp_b200_fun_jac.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 4
         L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
         L.kpp_b200_set_kernel.argtypes = [ctypes.c_int]
+        L.kpp_b200_rosenbrock_chain.argtypes = (
+            [ctypes.c_int, ctypes.c_int] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int]
+            + [_vp] * 2 + [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+            + [_vp] * 6)
 
     def _check(self, rc: int):
         if rc != KPP_B200_OK:
@@ -172,6 +176,40 @@ class Mechanism:
                 _vp(s.cuda_stream)))
         else:
             self._check(self.lib.kpp_b200_rosenbrock(*args, _vp(s.cuda_stream)))
+        return out
+
+    def rosenbrock_chain(self, var: torch.Tensor, fix: torch.Tensor, temp: torch.Tensor,
+                         tstart: torch.Tensor, dt: float, ncalls: int, atol: torch.Tensor,
+                         rtol: torch.Tensor, ipar: Sequence[int], rpar: Sequence[float],
+                         cfactor: Optional[torch.Tensor] = None,
+                         sun: Optional[torch.Tensor] = None,
+                         hstart: Optional[torch.Tensor] = None,
+                         order: Optional[torch.Tensor] = None, ncells: Optional[int] = None,
+                         out: Optional[RosenbrockResult] = None,
+                         stream: Optional[torch.cuda.Stream] = None) -> RosenbrockResult:
+        """The driver loop over INTEGRATE for every cell in one persistent
+        launch (kpp_b200_rosenbrock_chain): `ncalls` calls of `dt` seconds
+        from tstart, Hstart chained from Hexit, counters summed.  `order`
+        (int32 permutation) is the work-queue order.  Asynchronous."""
+        f64, i32 = torch.float64, torch.int32
+        self._dev(var, f64, "var")
+        ld = var.shape[1]
+        n = ld if ncells is None else ncells
+        for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (atol, "atol"),
+                      (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun"), (hstart, "hstart")):
+            self._dev(t, f64, nm)
+        self._dev(order, i32, "order")
+        if out is None:
+            out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
+                                   istatus=torch.empty(8, ld, dtype=i32, device=var.device),
+                                   rstatus=torch.empty(2, ld, dtype=f64, device=var.device))
+        ip = (ctypes.c_int * 20)(*[int(x) for x in ipar])
+        rp = (ctypes.c_double * 20)(*[float(x) for x in rpar])
+        s = stream if stream is not None else torch.cuda.current_stream(var.device)
+        self._check(self.lib.kpp_b200_rosenbrock_chain(
+            n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
+            float(dt), int(ncalls), _ptr(atol), _ptr(rtol), ip, rp, _ptr(hstart), _ptr(order),
+            _ptr(out.istatus), _ptr(out.rstatus), _ptr(out.ierr), _vp(s.cuda_stream)))
         return out
 
     @staticmethod

@@ -60,6 +60,14 @@ class Workload:
         t0 = self.tstart + k * self.dt
         return t0, t0 + self.dt
 
+    def driver_bounds(self, k: int):
+        """Bounds of call k of the reference driver loop, TIME += DT
+        (drv/general.c:59-76): the times kpp_b200_rosenbrock_chain uses."""
+        t0 = self.tstart.copy()
+        for _ in range(k):
+            t0 = t0 + self.dt
+        return t0, t0 + self.dt
+
     def subset(self, n: int) -> "Workload":
         """The first n cells (same values, same per-cell streams)."""
         sl = slice(0, n)

@@ -86,3 +86,22 @@ def test_controls_layouts():
     icntrl = [1, 0, 5, 500] + [0] * 16   # ICNTRL(3) = method, ICNTRL(4) = max steps
     rcntrl = [1e-3, 100.0, 1.0, 0.1, 5.0, 0.2, 0.8] + [0.0] * 13
     assert from_fortran(icntrl, rcntrl) == (ipar, rpar)
+
+
+def test_scheduler_library_exports_every_declared_entry():
+    """libkpp_b200_sched.so exports every function of include/kpp_sched.h and
+    loads without a GPU; creating a network without a GPU fails loudly."""
+    from kpp_b200.build import LIB
+    lib = LIB / "libkpp_b200_sched.so"
+    assert lib.exists(), "build the libraries first: python -m kpp_b200.build"
+    text = re.sub(r"/\*.*?\*/", "", (REPO / "include" / "kpp_sched.h").read_text(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(kpp_sched_\w+)\s*\(", text)))
+    assert "kpp_sched_plan" in names and len(names) >= 12
+    missing = [n for n in names if n not in exported(lib)]
+    assert not missing, missing
+    ctypes.CDLL(str(lib))
+    import torch
+    if not torch.cuda.is_available():
+        from kpp_b200.scheduler import Mlp, SchedError
+        with pytest.raises(SchedError):
+            Mlp(10)
