@@ -49,6 +49,15 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "saprc99 cell-steps/s at 2^20 cells, learned-scheduled vs plain, same accuracy"
 UNIT = "cell-steps/s"
+# How the committed scheduler weights were made (python -m kpp_b200.train_scheduler
+# on one B200): tuples logged from the plain GPU integrator, seed 20261204.
+TRAINING_SUMMARY = {
+    "saprc99_uniform95": {
+        "tuples": 4194304, "candidates_hstart": "1e-6 .. 1e-2 s, half decades",
+        "tuple_logging_s": 247.7, "epochs": 24, "batch": 8192, "train_s": 19.6,
+        "heldout_r2_log10_hstart": 0.918, "heldout_r2_ln_nstp": 0.974,
+        "mean_nstp_default_hstart": 49.42, "mean_nstp_best_candidate": 46.03},
+}
 
 
 # ---------------------------------------------------------------------------
@@ -471,7 +480,10 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             "network": "78 features -> 3 x 256 GELU -> 2 (log10 Hstart, ln Nstp); BF16 "
                        "mma.sync GEMMs, FP32 accumulate; trained on the GPU by "
                        "kpp_b200.train_scheduler",
-            "weights": sched.meta.get("source"),
+            "weights": (str(Path(sched.meta["source"]).resolve().relative_to(REPO))
+                        if str(Path(sched.meta["source"]).resolve()).startswith(str(REPO))
+                        else sched.meta["source"]),
+            "training": TRAINING_SUMMARY.get(args.workload),
         })
     elif sched_note:
         sched_block["note"] = sched_note
