@@ -531,11 +531,132 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     return result, wl
 
 
+def run_diurnal(args, rank, world, local_rank):
+    """The uneven-stiffness diurnal loop: every cell runs `--calls` chained
+    600 s chemistry steps (the reference driver loop, TIME += DT, STEPMIN =
+    Hexit) from its initial state.  Two forms, both replayed from CUDA graphs:
+      per-step  one kpp_b200_rosenbrock launch per chemistry step (a device
+                barrier between steps: every step waits for its slowest cell)
+      persistent  one kpp_b200_rosenbrock_chain launch: each warp takes 32
+                cells from the work queue and runs all their steps
+    Results are compared bit for bit; `value` is the persistent form."""
+    import torch
+    from kpp_b200 import load, workloads
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    mech = load(args.mech)
+    wname = args.workload if args.workload.endswith("classes") else "saprc99_classes"
+    wl = workloads.for_mechanism(mech, wname, args.ncells, seed=workloads.SEED_EVAL + rank)
+    n, ncalls = wl.ncells, args.calls
+    D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    var0 = D(wl.var)
+    fix, temp = D(wl.fix), D(wl.temp)
+    cf = D(wl.cfactor) if wl.cfactor is not None else None
+    sun = D(wl.sun) if wl.sun is not None else None
+    atol, rtol = D(wl.atol), D(wl.rtol)
+    bounds = [tuple(D(x) for x in wl.driver_bounds(k)) for k in range(ncalls)]
+    s = torch.cuda.Stream(dev)
+
+    var_a = var0.clone()
+    hs = torch.zeros(n, dtype=torch.float64, device=dev)
+    ist_a = torch.zeros(8, n, dtype=torch.int32, device=dev)
+    ierr_a = torch.ones(n, dtype=torch.int32, device=dev)
+    box = [None]
+
+    def per_step():
+        var_a.copy_(var0)
+        hs.zero_()  # first call: Hstart = RPAR[2] = 0, the default
+        for k in range(ncalls):
+            box[0] = o = mech.rosenbrock(var_a, fix, temp, bounds[k][0], bounds[k][1], atol,
+                                         rtol, wl.ipar, wl.rpar, cfactor=cf, sun=sun, hstart=hs,
+                                         out=box[0])
+            hs.copy_(o.rstatus[1])
+            if k == 0:
+                ist_a.copy_(o.istatus)
+                ierr_a.copy_(o.ierr)
+            else:
+                ist_a.add_(o.istatus)
+                torch.where(ierr_a == 1, o.ierr, ierr_a, out=ierr_a)
+
+    var_b = var0.clone()
+    box_b = [None]
+
+    def persistent():
+        var_b.copy_(var0)
+        box_b[0] = mech.rosenbrock_chain(var_b, fix, temp, bounds[0][0], wl.dt, ncalls, atol,
+                                         rtol, wl.ipar, wl.rpar, cfactor=cf, sun=sun,
+                                         out=box_b[0])
+
+    results = {}
+    for name, body in (("per_step", per_step), ("persistent", persistent)):
+        with torch.cuda.stream(s):
+            body()  # allocates the library workspace of stream s before capture
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            body()
+        # replay() launches on the current stream: time on that same stream
+        with torch.cuda.stream(s):
+            for _ in range(args.warmup):
+                g.replay()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with ClockSampler(local_rank) as clk:
+                e0.record(s)
+                for _ in range(args.steps):
+                    g.replay()
+                e1.record(s)
+                torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[name] = {"ms_per_loop": ms / args.steps,
+                         "value": world * n * ncalls * args.steps / (ms / 1e3),
+                         "clocks": clk.summary()}
+        del g
+    ob = box_b[0]
+    same = (torch.equal(var_a, var_b) and torch.equal(ist_a, ob.istatus)
+            and torch.equal(ierr_a, ob.ierr) and torch.equal(box[0].rstatus, ob.rstatus))
+    nstp = ob.istatus[2].to(torch.float64)
+    sza = wl.meta.get("sza")
+    classes = {}
+    if sza is not None:
+        for nm, lo, hi in (("day", 0, 85), ("terminator", 85, 95), ("night", 95, 181)):
+            mask = D(((sza >= lo) & (sza < hi)).astype(np.bool_))
+            if bool(mask.any()):
+                classes[nm] = float(nstp[mask].mean() / ncalls)
+    head = results["persistent"]
+    return {
+        "metric": f"{args.mech} cell-steps/s, {n} cells of uneven stiffness, {ncalls}-step "
+                  f"diurnal loop (persistent work queue vs one launch per step)",
+        "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_loop"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.mech} {wname}: 40 % day, 40 % night, 20 % within 5 deg "
+                               f"of the terminator; {ncalls} x {wl.dt:.0f} s Rodas3 steps, "
+                               f"RTOL 1e-3 ATOL 1e-2; one step = one diurnal loop of every cell",
+                   "cells_per_gpu": n, "graph": "both forms replayed from CUDA graphs",
+                   "l2": "inputs larger than L2"},
+        "impl": "kpp_b200", "gpu_launches": args.steps,
+        "per_step_launches": results["per_step"], "persistent": results["persistent"],
+        "persistent_speedup": results["persistent"]["value"] / results["per_step"]["value"],
+        "bit_identical": bool(same),
+        "internal_steps_per_cell_step": float(nstp.mean() / ncalls),
+        "internal_steps_per_cell_step_by_class": classes,
+        "ierr_ok_fraction": float((ob.ierr == 1).to(torch.float64).mean()),
+        "clocks": head["clocks"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--mode", choices=["fresh", "chain"], default="fresh")
+    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal"], default="fresh")
+    ap.add_argument("--calls", type=int, default=24, help="chemistry steps of a diurnal loop")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["kpp_b200", "reference"], default="kpp_b200")
     ap.add_argument("--mech", default="saprc99")
@@ -599,7 +720,13 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    result, wl = run_cuda_arm(args, rank, world, local_rank, pool)
+    if args.mode == "diurnal":
+        if pool is not None:
+            pool.close()
+            pool = None
+        result = run_diurnal(args, rank, world, local_rank)
+    else:
+        result, wl = run_cuda_arm(args, rank, world, local_rank, pool)
     if pool is not None:
         n_sample, _ = calibrated_sample(wl, procs, pool, target_s=args.cpu_seconds)
         rate, wall = cpu_reference_rate(wl, n_sample, procs, "", pool)
