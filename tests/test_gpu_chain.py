@@ -97,3 +97,36 @@ def test_chain_rejects_bad_arguments():
     with pytest.raises(KppError):
         m.rosenbrock_chain(dev(wl.var), dev(wl.fix), dev(wl.temp), dev(wl.tstart), wl.dt, 0,
                            dev(wl.atol), dev(wl.rtol), ipar, rpar)
+
+
+def test_chain_replays_from_a_cuda_graph():
+    """After one call on a stream (which allocates the workspace and queue
+    counter), the chained entry captures into a CUDA graph; replays give the
+    eager result."""
+    m = load("saprc99")
+    wl = workloads.for_mechanism(m, "saprc99_classes", 600, seed=8)
+    ipar, rpar = make_controls(method="rodas3", scalar_tol=True)
+    want = chained(m, wl, 3, ipar, rpar)
+    var0 = dev(wl.var)
+    var = var0.clone()
+    args = (dev(wl.fix), dev(wl.temp), dev(wl.tstart), wl.dt, 3, dev(wl.atol), dev(wl.rtol),
+            ipar, rpar)
+    kw = dict(cfactor=dev(wl.cfactor), sun=dev(wl.sun))
+    s = torch.cuda.Stream()
+    box = [None]
+
+    def body():
+        var.copy_(var0)
+        box[0] = m.rosenbrock_chain(var, *args, **kw, out=box[0])
+
+    with torch.cuda.stream(s):
+        body()
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        body()
+    for _ in range(2):
+        var.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        assert_same((var, box[0].istatus, box[0].rstatus, box[0].ierr), want)
