@@ -49,6 +49,15 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "saprc99 cell-steps/s at 2^20 cells, learned-scheduled vs plain, same accuracy"
 UNIT = "cell-steps/s"
+# DRAM traffic of the thread-per-cell Rosenbrock kernel per internal step
+# (ncu: 212.0 GB over 1.62 M internal steps, 32768 fresh saprc99 cells,
+# profiles/rosenbrock_kernel_thread_saprc99_32k_fresh.md): the per-cell work
+# set (LU factors, stage vectors) streams through L2 to HBM.
+DRAM_BYTES_PER_INTERNAL_STEP = 212.0e9 / 1.619e6
+# Compulsory bytes per cell-step: VAR in and out, FIX, TEMP, CFACTOR, SUN,
+# TSTART, TEND, Hstart in; ISTATUS, RSTATUS, IERR out (saprc99: 74 + 74 + 5 +
+# 6 doubles, 9 ints, 2 doubles).
+ALGO_BYTES_PER_CELL_STEP = (74 + 74 + 5 + 6) * 8 + 9 * 4 + 2 * 8
 # How the committed scheduler weights were made (python -m kpp_b200.train_scheduler
 # on one B200): tuples logged from the plain GPU integrator, seed 20261204.
 TRAINING_SUMMARY = {
@@ -291,6 +300,9 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             self.hs = torch.zeros(n, dtype=torch.float64, device=dev)
             self.hs_plan = torch.empty(n, dtype=torch.float64, device=dev)
             self.order = torch.empty(n, dtype=torch.int32, device=dev)
+            # events around the integration launch of each timed step (on the
+            # stream it runs on): the dominant kernel's own duration
+            self.kernel_events = {}
 
         def step(self, k):
             kk = 0 if fresh else k
@@ -298,16 +310,23 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                 var.copy_(var0)  # the same fresh batch every step
             t0, t1 = t_bounds[kk]
             warm = None if fresh else self.hs
+            ev = self.kernel_events[k] if self.kernel_events else None
             if not self.learned:
+                if ev:
+                    ev[0].record(stream)
                 self.out = mech.rosenbrock(var, fix, temp, t0, t1, atol, rtol, wl.ipar, wl.rpar,
                                            cfactor=cf, sun=sun, hstart=warm, out=self.out)
             else:
                 sched.plan(var, temp, t0, cfactor=cf, sun=sun, tend=t1, hstart=self.hs_plan,
                            order=self.order)
+                if ev:
+                    ev[0].record(stream)
                 self.out = mech.rosenbrock_chain(
                     var, fix, temp, t0, wl.dt, 1, atol, rtol, wl.ipar, wl.rpar, cfactor=cf,
                     sun=sun, hstart=self.hs_plan if fresh else warm, order=self.order,
                     out=self.out)
+            if ev:
+                ev[1].record(stream)
             if not fresh:
                 self.hs = self.out.rstatus[1].clone()
 
@@ -321,6 +340,9 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             self.snap_var = var.cpu().numpy() if not fresh else None
             self.snap_hs = self.hs.cpu().numpy().copy()
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            self.kernel_events = {k: (torch.cuda.Event(enable_timing=True),
+                                      torch.cuda.Event(enable_timing=True))
+                                  for k in range(args.warmup, total)}
             stats = []
             barrier()
             torch.cuda.synchronize()
@@ -333,6 +355,8 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                 torch.cuda.synchronize()
             barrier()
             self.ms = max_over_ranks(ev0.elapsed_time(ev1))
+            self.kernel_ms = sum(a.elapsed_time(b) for a, b in self.kernel_events.values())
+            self.kernel_events = {}
             self.clocks = clk.summary()
             self.ierr = self.out.ierr.cpu().numpy()
             self.var_out = var.cpu().numpy()
@@ -368,7 +392,9 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     fun_evals = nfun - (njac if fixed_rates else 0)   # dF/dT Fun elided for fixed rates
     flops = (fun_evals * opsd.get("fun", 0) + ndec * (opsd.get("jac", 0) + opsd.get("decomp", 0))
              + nsol * opsd.get("solve", 0) + nstp * vec["per_attempt"] + njac * vec["per_step"])
-    achieved_tflops = flops / (head.ms / 1e3) / 1e12
+    # the dominant kernel's launches only (the scheduling pass excluded)
+    achieved_tflops = flops / (head.kernel_ms / 1e3) / 1e12
+    traffic_per_launch = DRAM_BYTES_PER_INTERNAL_STEP * nstp / args.steps
     peak_fma, peak_muladd = fp64_peak(LIB / "libkpp_b200_util.so")
 
     # ---- end to end through the public API with host buffers (pinned host
@@ -520,7 +546,12 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         "stats": head.summary(),
         "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": peak_fma,
                      "unit": "TFLOP/s", "frac": achieved_tflops / peak_fma if peak_fma > 0 else None,
-                     "traffic": None,
+                     "traffic": traffic_per_launch,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                       "rosenbrock_kernel on 32768 fresh cells (profiles/), "
+                                       "per internal step, times this launch's internal steps",
+                     "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL_STEP * n,
+                     "kernel_ms_per_launch": head.kernel_ms / args.steps,
                      "peak_source": "measured on this GPU by the DFMA throughput kernel "
                                     "(kpp_b200/csrc/kpp_util.cu); MEASURED_PEAKS.json has no FP64 figure",
                      "peak_mul_add_tflops": peak_muladd,
