@@ -215,6 +215,14 @@ int kpp_b200_decomp_solve(int ncells, int ld, double *jvs, double *x,
 int kpp_b200_set_kernel(int which);
 int kpp_b200_get_kernel(void);
 
+/* Launch shape of the thread-per-cell kernel (process-wide): the number of
+ * 128-thread blocks per SM the Rosenbrock entries keep resident, 0 (the
+ * default) for as many as fit.  Fewer resident cells thrash L2 less; the
+ * autotuner (kpp_b200/autotune.py) picks the value per device and workload.
+ * Results do not depend on it.  No counterpart in the reference. */
+int kpp_b200_set_blocks_per_sm(int blocks);
+int kpp_b200_get_blocks_per_sm(void);
+
 /* Text of the last error of this thread's last failing call. */
 const char *kpp_b200_last_error(void);
 

@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <atomic>
 #include <mutex>
 
 #include "../../include/kpp_b200.h"
@@ -565,41 +566,69 @@ size_t warp_smem_bytes();
 // first failing call (1 when every call succeeds).  Failing calls do not stop
 // the loop, as the reference driver continues after INTEGRATE reports them.
 template <int METHOD, bool CHAIN, class W>
-__device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, int cell) {
+__device__ __forceinline__ void one_call(const LaunchArgs& a, W& w, const CellEnv& env, int cell,
+                                         int k, double& t0, double& rpar2) {
+  const long ld = a.ld;
+  const double t1 = CHAIN ? t0 + a.chain_dt : a.tend[cell];
+  Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
+  double texit = 0.0, hexit = 0.0;
+  const int ierr = rosenbrock_cell<METHOD>(env, w, t0, t1, a.atol, a.rtol, a, rpar2, st, texit,
+                                           hexit);
+  // y is untouched when the controls were rejected (IERR -1..-5); the
+  // statistics and Texit/Hexit are then zero, as IPAR/RPAR[10..] stay.
+  const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
+  if (!CHAIN || k == 0) {
+    a.ierr[cell] = ierr;
+#pragma unroll
+    for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
+  } else {
+    if (a.ierr[cell] == KPP_B200_IERR_SUCCESS) a.ierr[cell] = ierr;
+#pragma unroll
+    for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] += sv[i];
+  }
+  a.rstatus[cell] = texit;
+  a.rstatus[ld + cell] = hexit;
+  rpar2 = hexit;  // STEPMIN = RPAR[11]
+  t0 = t1;        // TIME += DT
+}
+
+// Integrates one cell: one Rosenbrock call over [tstart, tend] (grid-stride
+// launch, has = true), or, for the work queue, the driver loop of
+// drv/general.c:59-76 around INTEGRATE (int/rosenbrock.c:94-133): a.nchain
+// calls Rosenbrock(T, T + dt), T += dt, each call's Hstart = the previous
+// call's Hexit (STEPMIN), counters summed (INTEGRATE's Ns/Na/Nr/Ng),
+// Texit/Hexit of the last call, IERR of the first failing call (1 when every
+// call succeeds).  Failing calls do not stop the loop, as the reference
+// driver continues after INTEGRATE reports them.  In the queue form all 32
+// lanes of a warp call this together (has = false: no cell, the lane only
+// joins the barriers), and a warp barrier after each call starts the lanes'
+// next chemistry step together, so the lanes stay in the same phase of the
+// integrator instead of drifting apart over the calls.
+template <int METHOD, bool CHAIN, class W>
+__device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, int cell,
+                                                     bool has = true) {
   const long ld = a.ld;
   CellEnv env;
-  load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
+  double t0 = 0.0, rpar2 = 0.0;
+  if (has) {
+    load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
 #pragma unroll 4
-  for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
-
-  const int ncalls = CHAIN ? a.nchain : 1;
-  double t0 = a.tstart[cell];
-  double rpar2 = a.hstart ? a.hstart[cell] : a.rpar[2];
-  for (int k = 0; k < ncalls; k++) {
-    const double t1 = CHAIN ? t0 + a.chain_dt : a.tend[cell];
-    Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
-    double texit = 0.0, hexit = 0.0;
-    const int ierr = rosenbrock_cell<METHOD>(env, w, t0, t1, a.atol, a.rtol, a, rpar2, st,
-                                             texit, hexit);
-    // y is untouched when the controls were rejected (IERR -1..-5); the
-    // statistics and Texit/Hexit are then zero, as IPAR/RPAR[10..] stay.
-    const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
-    if (!CHAIN || k == 0) {
-      a.ierr[cell] = ierr;
-#pragma unroll
-      for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
-    } else {
-      if (a.ierr[cell] == KPP_B200_IERR_SUCCESS) a.ierr[cell] = ierr;
-#pragma unroll
-      for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] += sv[i];
-    }
-    a.rstatus[cell] = texit;
-    a.rstatus[ld + cell] = hexit;
-    rpar2 = hexit;  // STEPMIN = RPAR[11]
-    t0 = t1;        // TIME += DT
+    for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
+    t0 = a.tstart[cell];
+    rpar2 = a.hstart ? a.hstart[cell] : a.rpar[2];
   }
+  if (CHAIN) {
+    for (int k = 0; k < a.nchain; k++) {
+      if (has) one_call<METHOD, true>(a, w, env, cell, k, t0, rpar2);
+      __syncwarp();
+    }
+  } else {
+    one_call<METHOD, false>(a, w, env, cell, 0, t0, rpar2);
+  }
+  if (has) {
 #pragma unroll 4
-  for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+    for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+  }
 }
 
 // QUEUE = false: one thread slot integrates cells slot, slot + nslots, ...
@@ -626,7 +655,8 @@ rosenbrock_kernel(const LaunchArgs a) {
       base = __shfl_sync(0xffffffffu, base, 0);
       if (base >= a.ncells) break;  // warp-uniform
       const int pos = base + lane;
-      if (pos < a.ncells) integrate_cell_calls<METHOD, true>(a, w, a.order ? a.order[pos] : pos);
+      const bool has = pos < a.ncells;
+      integrate_cell_calls<METHOD, true>(a, w, has ? (a.order ? a.order[pos] : pos) : 0, has);
     }
   } else {
     for (long c = slot; c < a.ncells; c += a.nslots)
@@ -637,6 +667,14 @@ rosenbrock_kernel(const LaunchArgs a) {
 
 template <int M>
 int launch_method(LaunchArgs& a, int grid, cudaStream_t s) {
+  static bool l1_set = false;  // the kernel uses no shared memory: all of it as L1
+  if (!l1_set) {
+    cudaFuncSetAttribute(rosenbrock_kernel<M, true>,
+                         cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(rosenbrock_kernel<M, false>,
+                         cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    l1_set = true;
+  }
   if (a.queue)
     rosenbrock_kernel<M, true><<<grid, kBlock, 0, s>>>(a);
   else
@@ -797,24 +835,31 @@ constexpr bool kUsesScratch = false;
 // Thread slots a launch over ncells cells uses: one per cell, at most as many
 // as the device keeps resident (the rest of the cells are picked up by the
 // grid-stride loop), in whole blocks.
+// Blocks per SM the launches use: 0 = as many as can be resident.
+std::atomic<int> g_blocks_per_sm{0};
+
 long slots_for(int ncells) {
   static std::mutex mu;
-  static std::map<int, long> resident;  // device -> resident threads
+  static std::map<int, std::pair<int, int>> resident;  // device -> (SMs, blocks per SM)
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return kBlock;
-  long res;
+  int sms, per_sm;
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = resident.find(dev);
     if (it == resident.end()) {
-      int sms = 1, per_sm = 1;
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      per_sm = occupancy_method<4>();
-      if (per_sm < 1) per_sm = 1;
-      it = resident.emplace(dev, (long)sms * per_sm * kBlock).first;
+      int n = 1, b = 1;
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+      b = occupancy_method<4>();
+      if (b < 1) b = 1;
+      it = resident.emplace(dev, std::make_pair(n, b)).first;
     }
-    res = it->second;
+    sms = it->second.first;
+    per_sm = it->second.second;
   }
+  const int cap = g_blocks_per_sm.load();
+  if (cap > 0 && cap < per_sm) per_sm = cap;
+  long res = (long)sms * per_sm * kBlock;
   long want = ((long)ncells + kBlock - 1) / kBlock * kBlock;
   if (res > kSlotStride) res = kSlotStride;
   return want < res ? want : res;
@@ -1309,6 +1354,14 @@ int kpp_b200_set_kernel(int which) {
 }
 
 int kpp_b200_get_kernel(void) { return use_warp_kernel() ? 2 : 1; }
+
+int kpp_b200_set_blocks_per_sm(int blocks) {
+  if (blocks < 0 || blocks > 64) return fail(KPP_B200_EINVAL, "blocks per SM must be 0..64");
+  g_blocks_per_sm.store(blocks);
+  return KPP_B200_OK;
+}
+
+int kpp_b200_get_blocks_per_sm(void) { return g_blocks_per_sm.load(); }
 
 }  // extern "C"
 

@@ -93,6 +93,7 @@ class Mechanism:
         L.kpp_b200_fun_jac.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 4
         L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
         L.kpp_b200_set_kernel.argtypes = [ctypes.c_int]
+        L.kpp_b200_set_blocks_per_sm.argtypes = [ctypes.c_int]
         L.kpp_b200_rosenbrock_chain.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int]
             + [_vp] * 2 + [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
@@ -124,6 +125,14 @@ class Mechanism:
         """'auto', 'thread' (one thread per cell) or 'warp' (one warp per cell,
         work set in shared memory); both give bit-identical results."""
         self._check(self.lib.kpp_b200_set_kernel({"auto": 0, "thread": 1, "warp": 2}[which]))
+
+    def set_blocks_per_sm(self, blocks: int):
+        """Resident 128-thread blocks per SM of the thread-per-cell launches
+        (0: as many as fit); the results do not depend on it."""
+        self._check(self.lib.kpp_b200_set_blocks_per_sm(int(blocks)))
+
+    def blocks_per_sm(self) -> int:
+        return self.lib.kpp_b200_get_blocks_per_sm()
 
     def kernel(self) -> str:
         return {1: "thread", 2: "warp"}[self.lib.kpp_b200_get_kernel()]
