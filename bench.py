@@ -123,6 +123,30 @@ def host_cpu_model():
 
 
 # ---------------------------------------------------------------------------
+# multi-GPU plumbing: independent shards, device timing reduced by max
+# ---------------------------------------------------------------------------
+def shard_seed(rank: int) -> int:
+    """Each rank integrates its own shard of cells, drawn with the evaluation
+    seed + rank (no exchange of cell data between ranks)."""
+    from kpp_b200 import workloads
+    return workloads.SEED_EVAL + rank
+
+
+def reduce_max(value: float, device) -> float:
+    """The largest value over all ranks (the job ends with its slowest rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells_per_rank: int, world: int, steps: int, ms_max: float) -> float:
+    """cell-steps/s of the whole job: every rank's cells over the slowest rank's time."""
+    return world * cells_per_rank * steps / (ms_max / 1e3)
+
+
+# ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
@@ -251,8 +275,12 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
     mech.set_kernel(args.kernel)
+    shape = None
+    if args.kernel == "auto":
+        from kpp_b200 import autotune
+        shape = autotune.apply(mech, args.workload)  # tuned on this GPU, if recorded
     kernel = mech.kernel()
-    wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=workloads.SEED_EVAL + rank)
+    wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=shard_seed(rank))
     n = wl.ncells
     D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     var = D(wl.var)
@@ -282,12 +310,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             dist.barrier()
 
     def max_over_ranks(ms):
-        if world == 1:
-            return ms
-        import torch.distributed as dist
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ms if world == 1 else reduce_max(ms, dev)
 
     class Arm:
         """One way of running the steps: plain (grid-stride kernel, Hstart =
@@ -361,7 +384,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             self.ierr = self.out.ierr.cpu().numpy()
             self.var_out = var.cpu().numpy()
             self.ist = torch.stack(stats).sum(dim=0).cpu().numpy().astype(np.int64)
-            self.value = world * n * args.steps / (self.ms / 1e3)
+            self.value = whole_job_rate(n, world, args.steps, self.ms)
             return self
 
         def summary(self):
@@ -485,7 +508,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         ems = max_over_ranks((time.perf_counter() - t_start) * 1e3)
         barrier()
         same = bool(np.array_equal(h_var.numpy(), head.var_out))
-        e2e = {"value": world * n * args.steps / (ems / 1e3), "unit": UNIT,
+        e2e = {"value": whole_job_rate(n, world, args.steps, ems), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": ems / args.steps, "api": api, "matches_device_run": same}
 
@@ -536,6 +559,8 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                    "method": "rodas3", "scheduler": sched_block["kind"],
                    "parallelism": f"cell shards x{world}",
                    "kernel": {"thread": "thread per cell", "warp": "warp per cell"}[kernel],
+                   "launch_shape": shape or {"kernel": kernel, "blocks_per_sm": 0,
+                                             "source": "default (no tuning record)"},
                    "l2": "inputs larger than L2 (VAR alone %d MB)" % (wl.var.nbytes >> 20)},
         "impl": "kpp_b200",
         "gpu_launches": args.steps * (launches_learned if learned is not None
@@ -580,7 +605,7 @@ def run_diurnal(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
     wname = args.workload if args.workload.endswith("classes") else "saprc99_classes"
-    wl = workloads.for_mechanism(mech, wname, args.ncells, seed=workloads.SEED_EVAL + rank)
+    wl = workloads.for_mechanism(mech, wname, args.ncells, seed=shard_seed(rank))
     n, ncalls = wl.ncells, args.calls
     D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     var0 = D(wl.var)
@@ -666,12 +691,9 @@ def run_diurnal(args, rank, world, local_rank):
                 torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = reduce_max(ms, dev)
         results[name] = {"ms_per_loop": ms / args.steps,
-                         "value": world * n * ncalls * args.steps / (ms / 1e3),
+                         "value": whole_job_rate(n * ncalls, world, args.steps, ms),
                          "clocks": clk.summary()}
         del g
     ob = box_b[0]
