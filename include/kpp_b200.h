@@ -152,9 +152,11 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double *var, const double *fix,
  * a host model with a fixed device-memory budget, or a library that is handed
  * only its inputs and outputs).  The caller still passes every input and
  * output; the work arrays live in a fixed device array inside the library,
- * sized for at most 1024 cells per call (about 21 MB for saprc99, reserved on
- * every GPU that loads the library, until exit).  Larger batches are rejected
- * with KPP_B200_EINVAL; split them into calls of at most 1024 cells.
+ * sized for at most 1024 cells per call (about 21 MB for saprc99; 128 cells,
+ * 22 MB, for mechanisms whose per-cell work arrays would make 1024 cells
+ * exceed 64 MB, such as MCM isoprene), reserved on every GPU that loads the
+ * library, until exit.  Larger batches are rejected with KPP_B200_EINVAL;
+ * split them into calls of at most that many cells.
  * The first call on a device looks up that array's device address, so make it
  * before any stream capture.  No memory is allocated or freed by any call.
  * Every call uses the same array: calls that overlap on the GPU (concurrent

@@ -93,9 +93,24 @@ def build_kppcu(force: bool = False) -> Path:
     return exe
 
 
+# Mechanisms KPP ships for another target language only: their sources are
+# translated to a C-language KPP mechanism first (kpp_b200/gen/mcm.py).
+TRANSLATED = {"mcm_isoprene": ("examples/mcm", ("mcm_isoprene.eqn", "constants_mcm.f90",
+                                                "driver_mcm.f90"))}
+
+
 def mechanism_sources(mech: str, kpp_home: str):
     """Files kppcu reads for a mechanism (for the incremental-build hash)."""
     files = [MECH_DIR / f"{mech}.kpp"]
+    if mech in TRANSLATED:
+        sub, names = TRANSLATED[mech]
+        ex = Path(kpp_home) / sub if kpp_home else None
+        if ex and all((ex / n).exists() for n in names):
+            files += [ex / n for n in names] + [GEN_SRC / "fortran.py", GEN_SRC / "mcm.py"]
+            atoms = Path(kpp_home) / "models" / "atoms"
+            if atoms.exists():
+                files.append(atoms)
+        return files
     if kpp_home:
         for ext in (".def", ".spc", ".eqn"):
             p = Path(kpp_home) / "models" / f"{mech}{ext}"
@@ -119,7 +134,14 @@ def generate(mech: str, kpp_home: str, force: bool = False) -> Path | None:
     digest = _hash_files(src + [exe])
     if not force and stamp.exists() and stamp.read_text() == digest and (GEN_OUT / f"{mech}.cuh").exists():
         return GEN_OUT / f"{mech}.cuh"
-    _run([str(exe), str(MECH_DIR / f"{mech}.kpp"), "-o", str(out), "--home", kpp_home, "--root", mech])
+    top = MECH_DIR / f"{mech}.kpp"
+    if mech in TRANSLATED:
+        from .gen import mcm
+        src_dir = GEN_OUT / f"{mech}_src"
+        mcm.write(Path(kpp_home), src_dir)
+        shutil.copy(top, src_dir / top.name)
+        top = src_dir / top.name
+    _run([str(exe), str(top), "-o", str(out), "--home", kpp_home, "--root", mech])
     stamp.write_text(digest)
     return GEN_OUT / f"{mech}.cuh"
 

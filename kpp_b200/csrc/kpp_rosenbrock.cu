@@ -1013,7 +1013,10 @@ int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
 // that loads the library holds it until the process exits.  Host code must not
 // use the array's name as a device address (on the host it names a host-side
 // stand-in); static_scratch() obtains the device address per device.
-constexpr int kStaticMaxCells = 1024;
+// 1024 cells while that stays within 64 MB (saprc99: 21 MB); 128 cells for
+// mechanisms with larger per-cell work arrays (MCM isoprene: 22 MB).
+constexpr int kStaticMaxCells =
+    (kScratchPerSlot * 8L * 1024L <= (64L << 20)) ? 1024 : 128;
 static_assert(kStaticMaxCells % kBlock == 0, "whole blocks of thread slots");
 #if defined(KPP_SCRATCH)
 static __device__ __align__(256) double g_static_scratch[(size_t)kScratchPerSlot * kStaticMaxCells];

@@ -490,6 +490,13 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     std::snprintf(buf, sizeof buf, "%.17g", m.cfactor);
     o << "#undef KPP_CFACTOR\n#define KPP_CFACTOR " << buf << "\n\n";
   }
+  o << "// Large mechanisms call their unrolled rate, Fun, Jac_SP, LU and solve\n"
+       "// functions instead of inlining every call site: compile time grows with\n"
+       "// each inlined copy of a body of tens of thousands of operations, and one\n"
+       "// call is negligible next to such a body.\n"
+       "#ifndef KPP_MECH_INLINE\n"
+    << "#define KPP_MECH_INLINE " << (m.lu_nonzero >= 2000 ? "__noinline__" : "__forceinline__")
+    << "\n#endif\n\n";
   o << "// Species indices (variable species first, then fixed species).\n";
   for (int i = 0; i < nspec; i++) o << "#define ind_" << vw.name(i) << " " << i << "\n";
   for (int i = nvar; i < nspec; i++) o << "#define indf_" << vw.name(i) << " " << (i - nvar) << "\n";
@@ -559,7 +566,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   const char* names[3] = {"kpp_rconst_static", "kpp_rconst_sun", "kpp_rconst_dynamic"};
   for (int c = 0; c < 3; c++) {
     o << "template <class TR, class TV, class TF>\n"
-      << "__device__ __forceinline__ void " << names[c]
+      << "__device__ KPP_MECH_INLINE void " << names[c]
       << "(TR& RCONST, const double TIME, const double TEMP, const double CFACTOR,\n"
          "    double SUN, const TV& VAR, const TF& FIX) {\n"
          "  (void)TIME; (void)TEMP; (void)CFACTOR; (void)SUN; (void)VAR; (void)FIX;\n"
@@ -587,7 +594,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   // ---- Fun (aggregate form)
   o << "// ODE right-hand side Vdot = f(V) of one cell; A holds the equation rates.\n"
        "template <class TV, class TF, class TR, class TO, class TA>\n"
-       "__device__ __forceinline__ void kpp_fun(const TV& V, const TF& F, const TR& RCT,\n"
+       "__device__ KPP_MECH_INLINE void kpp_fun(const TV& V, const TF& F, const TR& RCT,\n"
        "    TO& Vdot, TA& A) {\n"
        "  (void)F; (void)RCT;\n";
   for (int j = 0; j < nr; j++) {
@@ -618,7 +625,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
        "// NEG = true writes its negation (the -Jac0 of ros_PrepareMatrix).  B holds\n"
        "// the partial derivatives of the equation rates (KPP_NJAC_TMP entries).\n"
        "template <bool NEG, class TV, class TF, class TR, class TJ, class TB>\n"
-       "__device__ __forceinline__ void kpp_jac_sp(const TV& V, const TF& F, const TR& RCT,\n"
+       "__device__ KPP_MECH_INLINE void kpp_jac_sp(const TV& V, const TF& F, const TR& RCT,\n"
        "    TJ& JVS, TB& B) {\n"
        "  (void)V; (void)F; (void)RCT;\n";
   for (int i = 0; i < nr; i++)
@@ -664,7 +671,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
          "// entry of row k is zero on entry to its elimination, 0 on success.\n"
          "template <class TJ>\n"
-         "__device__ __forceinline__ int kpp_decomp(TJ& JVS) {\n"
+         "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS) {\n"
          "  double a;\n";
     for (int k = 0; k < nvar; k++) {
       o << "  if (JVS[" << m.lu_diag[k] << "] == 0.0) return " << (k + 1) << ";\n";
@@ -686,7 +693,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   // ---- KppSolve, unrolled
   o << "// Solve (LU) x = b in place, b given in X.\n"
        "template <class TJ, class TX>\n"
-       "__device__ __forceinline__ void kpp_solve(const TJ& JVS, TX& X) {\n";
+       "__device__ KPP_MECH_INLINE void kpp_solve(const TJ& JVS, TX& X) {\n";
   for (int i = 0; i < nvar; i++) {
     int b = m.lu_crow[i], e = m.lu_diag[i];
     if (b < e) {

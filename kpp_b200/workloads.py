@@ -135,6 +135,36 @@ def saprc99(c_default: np.ndarray, cfactor_default: float, species: List[str], n
                     np.array([1e-3]), ipar, rpar, meta={"sza": angle, "pressure_hpa": p_hpa})
 
 
+# Initial mixing ratios of the MCM example driver (examples/mcm/driver_mcm.f90):
+# the species it sets, as fractions of M; every other species starts at zero.
+MCM_DRIVER_MIXING_RATIOS = {"O3": 3.0e-08, "NO2": 1.0e-10, "CH4": 1.8e-06, "C5H8": 1.0e-09}
+
+
+def mcm_isoprene(species: List[str], nvar: int, ncells: int, seed: int = SEED_EVAL,
+                 nsteps: int = 1, method: str = "rodas4") -> Workload:
+    """Config 4: log-normal concentrations (sigma 1, ln units) around the
+    example driver's initial mixing ratios times M, every other species at
+    the 1e-20 molec/cm3 floor; T uniform 250-310 K, p uniform 200-1013 hPa
+    (M = p / kT, the mechanism's CFACTOR), solar zenith angle uniform 0-90
+    degrees (SUN = its cosine); Rodas4, RTOL 1e-3, ATOL 1e-2, 300 s steps."""
+    rng = np.random.default_rng(seed)
+    temp = rng.uniform(250.0, 310.0, size=ncells)
+    p_hpa = rng.uniform(200.0, 1013.0, size=ncells)
+    m = p_hpa * 100.0 / (K_BOLTZMANN * temp) * 1e-6   # molec/cm3
+    frac = np.zeros(nvar)
+    for name, x in MCM_DRIVER_MIXING_RATIOS.items():
+        frac[[s.upper() for s in species[:nvar]].index(name)] = x
+    logn = rng.standard_normal(size=(nvar, ncells))
+    var = np.maximum(frac[:, None] * m[None, :] * np.exp(logn), 1e-20)
+    angle = rng.uniform(0.0, 90.0, size=ncells)
+    sun = np.cos(np.deg2rad(angle))
+    ipar, rpar = make_controls(method=method, scalar_tol=True)
+    return Workload("mcm_isoprene", "mcm_isoprene", ncells, np.ascontiguousarray(var),
+                    np.zeros((0, ncells)), temp, m, sun, np.full(ncells, 12 * 3600.0), 300.0,
+                    nsteps, np.array([1e-2]), np.array([1e-3]), ipar, rpar,
+                    meta={"sza": angle, "pressure_hpa": p_hpa})
+
+
 def for_mechanism(mech, name: str, ncells: int, seed: int = SEED_EVAL, **kw) -> Workload:
     """Workload `name` for a loaded kpp_b200.Mechanism (or anything exposing
     initial_values(), species and nvar)."""
@@ -145,4 +175,6 @@ def for_mechanism(mech, name: str, ncells: int, seed: int = SEED_EVAL, **kw) -> 
     if name.startswith("saprc99"):
         sza = "classes" if name.endswith("classes") else "uniform95"
         return saprc99(c, cf, list(mech.species), mech.nvar, ncells, seed, sza=sza, **kw)
+    if name == "mcm_isoprene":
+        return mcm_isoprene(list(mech.species), mech.nvar, ncells, seed, **kw)
     raise ValueError(name)

@@ -23,7 +23,7 @@ HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 KPP_REF="${KPP_REF:-/root/reference}"
 OUT="$HERE/_ref"
 MECHS=("$@")
-if [ ${#MECHS[@]} -eq 0 ]; then MECHS=(small_strato saprc99); fi
+if [ ${#MECHS[@]} -eq 0 ]; then MECHS=(small_strato saprc99 mcm_isoprene); fi
 
 if [ ! -d "$KPP_REF/src" ]; then
   echo "build_ref: reference sources not found at $KPP_REF; keeping prebuilt $OUT" >&2
@@ -51,15 +51,26 @@ for mech in "${MECHS[@]}"; do
   # the batch driver.  C_GLOBAL/C_RCONST add the optional per-cell SUN of the
   # batch driver: Update_RCONST runs the C_RCONST block before the rate
   # assignments (src/gen.c:2420-2435), after FunTemplate called Update_SUN.
+  # MCM isoprene: KPP ships it for Fortran 90 only; the mechanism is read from
+  # the C translation that the kpp_b200 build makes from examples/mcm
+  # (kpp_b200/gen/mcm.py), the same file kppcu reads.
+  model="#MODEL      $mech"
+  extras="#HESSIAN    ON
+#STOICMAT   ON"
+  if [ "$mech" = "mcm_isoprene" ]; then
+    (cd "$HERE/.." && python -m kpp_b200.gen.mcm --home "$KPP_REF" --out "$d" > /dev/null)
+    model=""
+    extras="#HESSIAN    OFF
+#STOICMAT   OFF"
+  fi
   cat > "$d/$mech.kpp" <<EOF
-#MODEL      $mech
+$model
 #LANGUAGE   C
 #DOUBLE     ON
 #INTEGRATOR rosenbrock
 #DRIVER     $HERE/refkpp/batch_driver
 #JACOBIAN   SPARSE_LU_ROW
-#HESSIAN    ON
-#STOICMAT   ON
+$extras
 #MEX        OFF
 #INLINE C_GLOBAL
   extern double kppref_sun_override;
@@ -71,6 +82,7 @@ for mech in "${MECHS[@]}"; do
   if (kppref_sun_ulps < 0) SUN = nextafter(SUN, -1.0);
 #ENDINLINE
 EOF
+  if [ "$mech" = "mcm_isoprene" ]; then echo "#INCLUDE    mcm_isoprene_c.eqn" >> "$d/$mech.kpp"; fi
   (cd "$d" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
     echo "build_ref: kpp failed for $mech" >&2; tail -20 "$d/kpp.log" >&2; exit 1; }
   srcs=()

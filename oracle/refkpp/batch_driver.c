@@ -75,7 +75,9 @@ static void set_cell_globals(int cell, int ld, const double *fix,
                              const double *sun, double t)
 {
   int i;
-  for (i = 0; i < NFIX; i++) FIX[i] = fix[(long)i * ld + cell];
+  /* NSPEC - NVAR real fixed species: with none, KPP still sets NFIX = 1 and
+     FIX[0] would lie past the end of C[NSPEC] */
+  for (i = 0; i < NSPEC - NVAR; i++) FIX[i] = fix[(long)i * ld + cell];
   TEMP = temp[cell];
   if (cfactor) CFACTOR = cfactor[cell];
   kppref_sun_override = sun ? sun[cell] : -1.0;
@@ -83,12 +85,15 @@ static void set_cell_globals(int cell, int ld, const double *fix,
 }
 
 /* Reaction-rate constants and ODE right-hand side / Jacobian of one cell at
-   time t, through the generated FunTemplate/JacTemplate path. */
+   time t, through the generated FunTemplate/JacTemplate path.  The cell's
+   concentrations are the model's VAR, as when INTEGRATE calls Rosenbrock:
+   rate constants that read the concentrations (Update_RCONST sees C) see
+   them. */
 int kppref_fun_jac(const double *var, const double *fix, double temp,
                    double cfactor, double sun, double t, double *rconst,
                    double *vdot, double *jvs)
 {
-  double y[NVAR];
+  double *y = VAR;
   int i;
   for (i = 0; i < NVAR; i++) y[i] = var[i];
   set_cell_globals(0, 1, fix, &temp, &cfactor, sun >= 0.0 ? &sun : 0, t);

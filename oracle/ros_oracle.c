@@ -5,7 +5,7 @@
  * path fails loudly when its CUDA library is missing instead of falling back
  * to any CPU code.
  *
- * What it is: a re-entrant, line-by-line restatement of the reference C
+ * What it is: a line-by-line restatement of the reference C
  * integrator int/rosenbrock.c together with the no-pivot sparse LU of
  * util/sutil.c:2-23, the BLAS-like helpers of util/blas.c it uses, and the
  * loop form of the generated KppSolve (src/gen.c:1960-2034).  It is compiled
@@ -478,7 +478,11 @@ int kppor_integrate(int ncells, int ld, double *var, const double *fix, const do
                     const double *tend, const double *atol, const double *rtol,
                     const int *ipar_in, const double *rpar_in, const double *hstart,
                     int *istatus, double *rstatus, int *ierr) {
-  double y[NVAR];
+  /* The cell is integrated in the model's VAR array, as INTEGRATE passes VAR
+     to Rosenbrock (int/rosenbrock.c:116): rate constants that read the
+     concentrations (Update_RCONST sees the global C) then see the accepted
+     state, exactly as in the reference. */
+  double *y = VAR;
   double rpar[20];
   int ipar[20];
   int cell, i;
@@ -487,7 +491,9 @@ int kppor_integrate(int ncells, int ld, double *var, const double *fix, const do
     for (i = 10; i < 20; i++) { ipar[i] = 0; rpar[i] = 0.0; }
     if (hstart) rpar[2] = hstart[cell];
     for (i = 0; i < NVAR; i++) y[i] = var[(long)i * ld + cell];
-    for (i = 0; i < NFIX; i++) FIX[i] = fix[(long)i * ld + cell];
+    /* NSPEC - NVAR real fixed species: with none, KPP still sets NFIX = 1
+       and FIX[0] would lie past the end of C[NSPEC] */
+    for (i = 0; i < NSPEC - NVAR; i++) FIX[i] = fix[(long)i * ld + cell];
     TEMP = temp[cell];
     if (cfactor) CFACTOR = cfactor[cell];
     kppref_sun_override = sun ? sun[cell] : -1.0;

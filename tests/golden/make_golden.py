@@ -120,6 +120,15 @@ def main():
     np.savez_compressed(HERE / "funjac_saprc99.npz", **funjac(o, wl, 6, wl.tstart))
     np.savez_compressed(HERE / "integrate_saprc99.npz",
                         **integrate_chain(o, wl, 2))
+    # MCM isoprene (translated from examples/mcm): 8 cells, 2 chained
+    # Rodas4 steps of 300 s
+    o = OracleLib("mcm_isoprene")
+    st = structure(o)
+    st["nfix"] = o.nspec - o.nvar  # KPP's C model pads NFIX to 1 when it is 0
+    (HERE / "structure_mcm_isoprene.json").write_text(json.dumps(st, indent=1))
+    wl = workloads.for_mechanism(_MechView(o), "mcm_isoprene", 8)
+    np.savez_compressed(HERE / "funjac_mcm_isoprene.npz", **funjac(o, wl, 3, wl.tstart))
+    np.savez_compressed(HERE / "integrate_mcm_isoprene.npz", **integrate_chain(o, wl, 2))
     for p in sorted(HERE.glob("*.*")):
         print(p.name, p.stat().st_size)
 

@@ -8,6 +8,7 @@
 #define __device__
 #define __host__
 #define __forceinline__ inline
+#define __noinline__
 #include <cmath>
 using std::cos;
 using std::exp;

@@ -26,7 +26,7 @@ def lib_path(mech: str, opt: str = "") -> Path:
     return REF_DIR / mech / f"libkppref_{mech}{opt}.so"
 
 
-def ensure_built(mechs=("small_strato", "saprc99")) -> bool:
+def ensure_built(mechs=("small_strato", "saprc99", "mcm_isoprene")) -> bool:
     """Build the oracle when its libraries are missing and the reference
     sources are present; True when every library exists afterwards."""
     if all(lib_path(m).exists() for m in mechs):

@@ -12,7 +12,7 @@ import pytest
 from kpp_b200 import Mechanism, from_fortran, library_path, make_controls
 from oracle_lib import REPO
 
-MECHS = ["small_strato", "saprc99"]
+MECHS = ["small_strato", "saprc99", "mcm_isoprene"]
 HEADER = REPO / "include" / "kpp_b200.h"
 
 

@@ -52,6 +52,23 @@ def test_structure_matches_reference_golden(kppcu, mech, tmp_path, golden_dir):
         assert got[k] == g[k], k
 
 
+HAVE_MCM = (Path(KPP_HOME) / "examples" / "mcm" / "mcm_isoprene.eqn").exists()
+
+
+@pytest.mark.skipif(not HAVE_MCM, reason="MCM example sources not present")
+def test_mcm_translation_structure_matches_reference_golden(kppcu, tmp_path, golden_dir):
+    """MCM isoprene through the Fortran-to-C translation and kppcu: species
+    order and LU pattern of the reference generator run on the same file."""
+    from kpp_b200.gen import mcm
+    mcm.write(Path(KPP_HOME), tmp_path)
+    shutil.copy(REPO / "kpp_b200" / "mechanisms" / "mcm_isoprene.kpp", tmp_path)
+    got = run_kppcu(kppcu, tmp_path / "mcm_isoprene.kpp", tmp_path / "out")
+    g = json.loads((golden_dir / "structure_mcm_isoprene.json").read_text())
+    assert got["species"] == g["species"]
+    for k in ("nvar", "nfix", "nreact", "lu_nonzero", "lu_irow", "lu_icol", "lu_crow", "lu_diag"):
+        assert got[k] == g[k], k
+
+
 # Small mechanisms in the KPP language exercising the front end.
 SMALL = {
     "toy_chain": """
@@ -142,7 +159,7 @@ def _p(a):
 
 
 @pytest.mark.skipif(not ensure_built(), reason="oracle libraries not built")
-@pytest.mark.parametrize("mech", MECHS)
+@pytest.mark.parametrize("mech", MECHS + ["mcm_isoprene"])
 def test_emitted_arithmetic_bit_identical_on_host(mech, tmp_path, golden_dir):
     h = _host_lib(mech, tmp_path)
     o = OracleLib(mech)
