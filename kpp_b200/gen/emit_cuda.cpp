@@ -28,7 +28,9 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <set>
 #include <sstream>
+#include <vector>
 
 #include "mechanism.hpp"
 
@@ -200,13 +202,50 @@ void emit_int_table(std::ostream& o, const char* name, const std::vector<int>& v
 
 enum RateClass { RC_STATIC = 0, RC_SUN = 1, RC_DYNAMIC = 2 };
 
+// Names declared by `double ...;` statements of an inline block (the
+// variables it makes available to the rate expressions).
+std::set<std::string> declared_names(const std::string& code) {
+  std::set<std::string> out;
+  size_t p = 0;
+  while ((p = code.find("double", p)) != std::string::npos) {
+    bool word_start = p == 0 || !(std::isalnum((unsigned char)code[p - 1]) || code[p - 1] == '_');
+    size_t q = p + 6;
+    p = q;
+    if (!word_start || q >= code.size() || !std::isspace((unsigned char)code[q])) continue;
+    size_t end = code.find(';', q);
+    if (end == std::string::npos) break;
+    std::string decl = code.substr(q, end - q);
+    int depth = 0;
+    bool want = true;
+    for (size_t i = 0; i < decl.size(); i++) {
+      char c = decl[i];
+      if (c == '(' || c == '[') depth++;
+      else if (c == ')' || c == ']') depth--;
+      else if (c == ',' && depth == 0) want = true;
+      else if (c == '=' && depth == 0) want = false;
+      else if (want && (std::isalpha((unsigned char)c) || c == '_')) {
+        size_t b = i;
+        while (i < decl.size() && (std::isalnum((unsigned char)decl[i]) || decl[i] == '_')) i++;
+        out.insert(decl.substr(b, i - b));
+        want = false;
+        i--;
+      }
+    }
+    p = end;
+  }
+  return out;
+}
+
 // What a rate expression depends on: only TEMP/CFACTOR and pure functions
 // (static for a cell), also SUN, or anything else (time, concentrations,
 // user variables: recomputed at every evaluation).
-int classify_rate(const std::string& e) {
+int classify_rate(const std::string& e, const std::set<std::string>& static_names = {},
+                  const std::set<std::string>& sun_names = {}) {
   static const char* pure[] = {"ARR_abc", "ARR_ab", "ARR_ac", "EP2", "EP3", "FALL", "exp",
                                "pow", "log", "log10", "sqrt", "cos", "sin", "tan", "fabs",
-                               "fmin", "fmax", "TEMP", "CFACTOR", "double", "float"};
+                               "fmin", "fmax", "expf", "powf", "logf", "log10f", "sqrtf",
+                               "cosf", "sinf", "tanf", "fabsf", "fminf", "fmaxf", "TEMP",
+                               "CFACTOR", "double", "float"};
   int cls = RC_STATIC;
   size_t i = 0;
   while (i < e.size()) {
@@ -221,6 +260,7 @@ int classify_rate(const std::string& e) {
           while (i < e.size() && std::isdigit((unsigned char)e[i])) i++;
         }
       }
+      if (i < e.size() && std::strchr("fFlL", e[i])) i++;  // C literal suffix
       continue;
     }
     if (std::isalpha((unsigned char)c) || c == '_') {
@@ -230,8 +270,8 @@ int classify_rate(const std::string& e) {
       bool known = false;
       for (const char* p : pure)
         if (id == p) known = true;
-      if (known) continue;
-      if (id == "SUN") cls = std::max(cls, (int)RC_SUN);
+      if (known || static_names.count(id)) continue;
+      if (id == "SUN" || sun_names.count(id)) cls = std::max(cls, (int)RC_SUN);
       else cls = RC_DYNAMIC;
       continue;
     }
@@ -538,11 +578,24 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   // recomputes it, so hoisting a rate out of the time loop when its inputs
   // are constant for the cell gives the same bits.
   std::vector<int> rclass(nr, RC_STATIC);
-  bool rconst_inline = m.inline_code.count("CUDA_RCONST") > 0;
+  // Inline rate prologues: CUDA_RCONST_STATIC (depends on TEMP / CFACTOR
+  // only) and CUDA_RCONST_SUN (also on SUN) declare names a rate may use
+  // without leaving that class; CUDA_RCONST alone (code of unknown
+  // dependence) makes every rate dynamic.
+  auto inl = [&](const char* k) {
+    auto it = m.inline_code.find(k);
+    return it == m.inline_code.end() ? std::string() : it->second;
+  };
+  const std::string inl_static = inl("CUDA_RCONST_STATIC"), inl_sun = inl("CUDA_RCONST_SUN"),
+                    inl_dyn = inl("CUDA_RCONST");
+  const bool classed = !inl_static.empty() || !inl_sun.empty();
+  const bool rconst_inline = !inl_dyn.empty() && !classed;
+  const std::set<std::string> static_names = declared_names(inl_static);
+  const std::set<std::string> sun_names = declared_names(inl_sun);
   for (int j = 0; j < nr; j++) {
     const Reaction& r = m.reactions[j];
     if (r.kind == RATE_NUMBER) { rclass[j] = -1; continue; }
-    rclass[j] = rconst_inline ? RC_DYNAMIC : classify_rate(r.rate);
+    rclass[j] = rconst_inline ? RC_DYNAMIC : classify_rate(r.rate, static_names, sun_names);
   }
   const char* kRateMacros =
       "#define ARR_abc(a0, b0, c0) kpp_arr_abc(TEMP, (float)(a0), (float)(b0), (float)(c0))\n"
@@ -571,8 +624,9 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
          "    double SUN, const TV& VAR, const TF& FIX) {\n"
          "  (void)TIME; (void)TEMP; (void)CFACTOR; (void)SUN; (void)VAR; (void)FIX;\n"
       << kRateMacros;
-    if (c == RC_DYNAMIC && rconst_inline)
-      o << "  // #INLINE CUDA_RCONST\n" << m.inline_code.at("CUDA_RCONST") << "\n";
+    if (!inl_static.empty()) o << "  // #INLINE CUDA_RCONST_STATIC\n" << inl_static << "\n";
+    if (c >= RC_SUN && !inl_sun.empty()) o << "  // #INLINE CUDA_RCONST_SUN\n" << inl_sun << "\n";
+    if (c == RC_DYNAMIC && !inl_dyn.empty()) o << "  // #INLINE CUDA_RCONST\n" << inl_dyn << "\n";
     for (int j = 0; j < nr; j++) {
       if (rclass[j] == c) o << "  RCONST[" << j << "] = (" << m.reactions[j].rate << ");\n";
       // constant rates are folded into Fun/Jac_SP; the reference's
@@ -668,26 +722,67 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   {
     std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
     for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
-    o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
-         "// entry of row k is zero on entry to its elimination, 0 on success.\n"
-         "template <class TJ>\n"
-         "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS) {\n"
-         "  double a;\n";
-    for (int k = 0; k < nvar; k++) {
-      o << "  if (JVS[" << m.lu_diag[k] << "] == 0.0) return " << (k + 1) << ";\n";
-      for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
-        int j = m.lu_icol[kk];
-        ops_decomp += 1;
-        o << "  a = -JVS[" << kk << "] / JVS[" << m.lu_diag[j] << "];\n";
-        o << "  JVS[" << kk << "] = -a;\n";
-        for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
-          int t = pos[k][m.lu_icol[jj]];
-          ops_decomp += 2;
-          o << "  JVS[" << t << "] = JVS[" << t << "] + a*JVS[" << jj << "];\n";
+    // Large mechanisms: the rows in chunks of about kChunkOps operations, one
+    // function each, called in row order (the same operations in the same
+    // order); a single straight-line body of tens of thousands of operations
+    // makes the device assembler's time grow much faster than its length.
+    const bool chunked = m.lu_nonzero >= 2000;
+    const int kChunkOps = 2500;
+    std::vector<int> starts = {0};
+    if (chunked) {
+      int acc = 0;
+      for (int k = 0; k < nvar; k++) {
+        int row_ops = 0;
+        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+          int j = m.lu_icol[kk];
+          row_ops += 1 + 2 * (m.lu_crow[j + 1] - m.lu_diag[j] - 1);
         }
+        if (acc > 0 && acc + row_ops > kChunkOps) {
+          starts.push_back(k);
+          acc = 0;
+        }
+        acc += row_ops;
       }
     }
-    o << "  return 0;\n}\n\n";
+    starts.push_back(nvar);
+    const int nchunks = (int)starts.size() - 1;
+    for (int c = 0; c < nchunks; c++) {
+      if (nchunks > 1)
+        o << "// Rows " << starts[c] << ".." << starts[c + 1] - 1 << " of the LU.\n"
+          << "template <class TJ>\n"
+          << "__device__ __noinline__ int kpp_decomp_rows" << c << "(TJ& JVS) {\n";
+      else
+        o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
+             "// entry of row k is zero on entry to its elimination, 0 on success.\n"
+             "template <class TJ>\n"
+             "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS) {\n";
+      o << "  double a;\n";
+      for (int k = starts[c]; k < starts[c + 1]; k++) {
+        o << "  if (JVS[" << m.lu_diag[k] << "] == 0.0) return " << (k + 1) << ";\n";
+        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+          int j = m.lu_icol[kk];
+          ops_decomp += 1;
+          o << "  a = -JVS[" << kk << "] / JVS[" << m.lu_diag[j] << "];\n";
+          o << "  JVS[" << kk << "] = -a;\n";
+          for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
+            int t = pos[k][m.lu_icol[jj]];
+            ops_decomp += 2;
+            o << "  JVS[" << t << "] = JVS[" << t << "] + a*JVS[" << jj << "];\n";
+          }
+        }
+      }
+      o << "  (void)a;\n  return 0;\n}\n\n";
+    }
+    if (nchunks > 1) {
+      o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
+           "// entry of row k is zero on entry to its elimination, 0 on success.\n"
+           "template <class TJ>\n"
+           "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS) {\n"
+           "  int r;\n";
+      for (int c = 0; c < nchunks; c++)
+        o << "  if ((r = kpp_decomp_rows" << c << "(JVS)) != 0) return r;\n";
+      o << "  return 0;\n}\n\n";
+    }
   }
 
   // ---- KppSolve, unrolled

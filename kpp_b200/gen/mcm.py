@@ -8,10 +8,11 @@ RO2 sum over the peroxy radicals in an `#INLINE F90_RCONST` block; the
 example driver (driver_mcm.f90) sets M, O2, N2 and H2O.  This module writes,
 from those files, the same species and equations with every rate translated
 to C (kpp_b200/gen/fortran.py, Fortran literal kinds and precedence kept)
-and an `#INLINE CUDA_RCONST` (`mcm_isoprene_cuda.eqn`, for kppcu) or
-`C_RCONST` block (`mcm_isoprene_c.eqn`, for the reference generator) that
-computes, per cell and per rate evaluation, what the Fortran module and
-driver compute:
+and inline rate prologues (`mcm_isoprene_cuda.eqn` for kppcu: split into
+CUDA_RCONST_STATIC / _SUN / CUDA_RCONST by dependence, so that kppcu hoists
+the rates that do not read the concentrations; `mcm_isoprene_c.eqn` for the
+reference generator: one C_RCONST block) that compute, per cell, what the
+Fortran module and driver compute:
 
   M = CFACTOR (molec/cm3, per cell); O2, N2, H2O from M as the driver does;
   cos(zenith) = SUN (per cell; the J formulas only use cos(zenith));
@@ -77,39 +78,48 @@ def _inline_blocks(eqn: str):
     return pat.sub("", eqn), ro2
 
 
-def rconst_code(constants_src: str, driver_src: str, ro2_stmts: list, lang: str) -> str:
-    """The per-cell rate-constant prologue in C (`lang` 'C': the reference's
-    global C array; 'CUDA': the VAR accessor of the device rate functions)."""
+def rconst_parts(constants_src: str, driver_src: str, ro2_stmts: list, lang: str):
+    """The per-cell rate-constant prologue in C, split by what it depends on:
+    (TEMP / CFACTOR only: M, O2, N2, H2O and the named constants; SUN: the
+    photolysis frequencies J; the concentrations: RO2).  `lang` 'C' reads the
+    reference's global C array, 'CUDA' the VAR accessor of the device rate
+    functions."""
     jp = _j_params(constants_src)
     nj = max(jp.values()) + 1 if jp else 1
     conc = "C" if lang == "C" else "VAR"
     ctx = Context(arrays={"J": lambda n, i: f"J[{i.text}]",
                           "C": lambda n, i: f"{conc}[{i.text}]"},
                   int_params=jp)
-    lines = ["  /* MCM rate-constant environment of the cell, translated from",
-             "     examples/mcm/constants_mcm.f90 and driver_mcm.f90 */",
-             "  double M = CFACTOR;"]
+    static = ["  /* MCM rate-constant environment of the cell, translated from",
+              "     examples/mcm/constants_mcm.f90 and driver_mcm.f90 */",
+              "  double M = CFACTOR;"]
     for st in _driver_env(driver_src):
         c, name = translate_assignment(st, ctx)
-        lines.append(f"  double {c}")
-    names, body = [], []
+        static.append(f"  double {c}")
+    names, kbody, jbody = [], [], []
     for st in _constants_body(constants_src):
         st = re.sub(r"cos\s*\(\s*zenith\s*\)", "SUN", st, flags=re.I)
         if re.search(r"\bzenith\b", st, re.I):
             raise FortranError(f"zenith used other than as cos(zenith): {st}")
         c, name = translate_assignment(st, ctx)
-        if name.upper() != "J" and name not in names:
+        if name.upper() == "J":
+            jbody.append("  " + c)
+            continue
+        if re.search(r"\bSUN\b|\bJ\s*\(", st):
+            raise FortranError(f"a named constant depends on the sun: {st}")
+        if name not in names:
             names.append(name)
-        body.append("  " + c)
-    lines.append(f"  double J[{nj}];")
+        kbody.append("  " + c)
     for k in range(0, len(names), 8):
-        lines.append("  double " + ", ".join(names[k:k + 8]) + ";")
-    lines += body
+        static.append("  double " + ", ".join(names[k:k + 8]) + ";")
+    static += kbody
+    static.append("  (void)M;" + "".join(f" (void){n};" for n in DRIVER_ENV))
+    sun = [f"  double J[{nj}];"] + jbody + ["  (void)J;"]
+    dyn = []
     for st in ro2_stmts:
-        lines += _sum_lines(st, conc)
-    # every name may be unused by some rate: keep compilers quiet
-    lines.append("  (void)M; (void)J; (void)RO2;" + "".join(f" (void){n};" for n in DRIVER_ENV))
-    return "\n".join(lines) + "\n"
+        dyn += _sum_lines(st, conc)
+    dyn.append("  (void)RO2;")
+    return ("\n".join(static) + "\n", "\n".join(sun) + "\n", "\n".join(dyn) + "\n")
 
 
 def _sum_lines(stmt: str, conc: str, per_line: int = 6) -> list:
@@ -181,13 +191,20 @@ def write(home: Path, out_dir: Path) -> Path:
     out_dir.mkdir(parents=True, exist_ok=True)
     for name, text, lang in (("mcm_isoprene_cuda.eqn", full, "CUDA"),
                              ("mcm_isoprene_c.eqn", ref, "C")):
-        block = rconst_code(constants, driver, ro2, lang)
+        st, sn, dy = rconst_parts(constants, driver, ro2, lang)
         if lang == "C":
-            block += f"  double MCMR[{len(rates)}];\n"
-            block += "".join(f"  MCMR[{k}] = {r};\n" for k, r in enumerate(rates))
+            # the reference evaluates everything in Update_RCONST, in order
+            blocks = (f"#INLINE C_RCONST\n{st}{sn}{dy}  double MCMR[{len(rates)}];\n"
+                      + "".join(f"  MCMR[{k}] = {r};\n" for k, r in enumerate(rates))
+                      + "#ENDINLINE\n")
+        else:
+            # kppcu hoists rates by class: a rate using only the static names
+            # is computed once per cell, one using J once per SUN value
+            blocks = (f"#INLINE CUDA_RCONST_STATIC\n{st}#ENDINLINE\n"
+                      f"#INLINE CUDA_RCONST_SUN\n{sn}#ENDINLINE\n"
+                      f"#INLINE CUDA_RCONST\n{dy}#ENDINLINE\n")
         i = text.upper().index("#EQUATIONS")
-        (out_dir / name).write_text(head + text[:i] + f"#INLINE {lang}_RCONST\n{block}"
-                                    "#ENDINLINE\n" + text[i:])
+        (out_dir / name).write_text(head + text[:i] + blocks + text[i:])
     return out_dir / "mcm_isoprene_cuda.eqn"
 
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 import torch
 
-from kpp_b200 import load, make_controls, workloads
+from kpp_b200 import make_controls, workloads
 from parity import FUNJAC_REL_TOL, REL_TOL, assert_var_parity, max_rel_err, rel_err_funjac
 
 pytestmark = pytest.mark.gpu
@@ -19,6 +19,15 @@ MECHS = ["small_strato", "saprc99", "mcm_isoprene"]
 
 def dev(a, dtype=torch.float64):
     return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def load(mech):
+    """The mechanism's library; mechanisms built only on request (see
+    kpp_b200.build.ON_REQUEST) are skipped when their library is absent."""
+    from kpp_b200 import build, load as _load
+    if mech in build.ON_REQUEST and not build.library_path(mech).exists():
+        pytest.skip(f"{mech} is built on request: python -m kpp_b200.build {mech}")
+    return _load(mech)
 
 
 def alternates(*a, **k):
