@@ -225,6 +225,27 @@ int kpp_b200_get_kernel(void);
 int kpp_b200_set_blocks_per_sm(int blocks);
 int kpp_b200_get_blocks_per_sm(void);
 
+/* Host-model species order (GenerateShuffle_user2kpp / _kpp2user,
+ * src/gen.c:3401-3468): user species k is the k-th species the mechanism
+ * declares as variable, unused ones included, among its first NSPEC - 1
+ * declared species (the reference's loop bound); kpp_index[k] is its index
+ * in the library's VAR order, or -1 when it takes no part in the mechanism
+ * (or k >= NVAR, where the reference's shuffle stops).  *nuser receives the
+ * number of user species; either pointer may be NULL. */
+int kpp_b200_user_species(int *nuser, int *kpp_index);
+
+/* Batched Shuffle_user2kpp: var[kpp_index[k]][c] = v_user[k][c] for every
+ * mapped user species k (v_user [nuser][ld_user], var [NVAR][ld], cell index
+ * fastest); other VAR rows are left as they are.  Device pointers,
+ * asynchronous. */
+int kpp_b200_shuffle_user2kpp(int ncells, int ld_user, const double *v_user, int ld,
+                              double *var, void *stream);
+
+/* Batched Shuffle_kpp2user: v_user[k][c] = var[kpp_index[k]][c] for every
+ * mapped user species k; unmapped rows of v_user are left as they are. */
+int kpp_b200_shuffle_kpp2user(int ncells, int ld, const double *var, int ld_user,
+                              double *v_user, void *stream);
+
 /* Text of the last error of this thread's last failing call. */
 const char *kpp_b200_last_error(void);
 

@@ -151,6 +151,10 @@ def library_path(mech: str) -> Path:
 
 
 def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> Path:
+    """nvcc each part (the C ABI, one part per Rosenbrock method) in parallel
+    and link the shared library.  A part is recompiled only when its own
+    preprocessed source or flags change (large mechanisms take many minutes
+    per part), so a change confined to the C ABI rebuilds part 0 alone."""
     LIB.mkdir(exist_ok=True)
     objdir = BUILD / mech
     objdir.mkdir(parents=True, exist_ok=True)
@@ -158,25 +162,41 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> 
     defines = [f'-DKPP_MECH_HEADER="{header}"']
     if meta["lu_nonzero"] >= SCRATCH_LU_NONZERO:
         defines.append("-DKPP_SCRATCH")
-    srcs = [CSRC / "kpp_rosenbrock.cu", CSRC / "kpp_ratelaws.cuh", CSRC / "kpp_warp.cuh", header,
-            INCLUDE / "kpp_b200.h"]
-    digest = _hash_files(srcs, " ".join(ARCH + NVCC_FLAGS + defines))
+    host_header = GEN_OUT / f"{mech}_host.h"
     lib = library_path(mech)
-    stamp = objdir / "lib.stamp"
-    if not force and lib.exists() and stamp.exists() and stamp.read_text() == digest:
-        return lib
     parts = [0] + METHOD_PARTS
 
-    def compile_part(part: int) -> Path:
+    def part_flags(part: int):
+        f = ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT)]
+        if part == 0 and host_header.exists():
+            f.append(f'-DKPP_HOST_HEADER="{host_header}"')
+        return f
+
+    def compile_part(part: int):
         obj = objdir / f"part{part}.o"
-        _run([nvcc()] + ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT),
-              "-c", str(CSRC / "kpp_rosenbrock.cu"), "-o", str(obj)])
-        return obj
+        flags = part_flags(part)
+        pre = subprocess.run([nvcc(), "-E"] + flags + [str(CSRC / "kpp_rosenbrock.cu")],
+                             capture_output=True, check=True).stdout
+        # the code only: line markers and blank lines (comments are already
+        # gone) do not change what is compiled
+        code = b"\n".join(ln for ln in pre.splitlines()
+                           if ln.strip() and not ln.lstrip().startswith(b"#"))
+        digest = hashlib.sha256(code + " ".join(flags).encode()).hexdigest()
+        stamp = objdir / f"part{part}.stamp"
+        if not force and obj.exists() and stamp.exists() and stamp.read_text() == digest:
+            return obj, False
+        _run([nvcc()] + flags + ["-c", str(CSRC / "kpp_rosenbrock.cu"), "-o", str(obj)])
+        stamp.write_text(digest)
+        return obj, True
 
     with cf.ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
-        objs = list(ex.map(compile_part, parts))
-    _run([nvcc()] + ARCH + ["-shared", "-o", str(lib)] + [str(o) for o in objs] + ["-lcudart"])
-    stamp.write_text(digest)
+        results = list(ex.map(compile_part, parts))
+    if any(rebuilt for _, rebuilt in results) or not lib.exists():
+        _run([nvcc()] + ARCH + ["-shared", "-o", str(lib)] + [str(o) for o, _ in results]
+             + ["-lcudart"])
+    params = GEN_OUT / f"{mech}_Parameters.h"
+    if params.exists():
+        shutil.copy(params, LIB / f"kpp_b200_{mech}_Parameters.h")
     return lib
 
 

@@ -1176,9 +1176,77 @@ int host_pipeline(int ncells, int ld, double* var, const double* fix, const doub
 }  // namespace kpp_b200_impl
 
 #if KPP_PART == 0
+#ifdef KPP_HOST_HEADER
+#include KPP_HOST_HEADER
+#else
+#define KPP_NUSER 0
+namespace kpp_host {
+static const int kUserToKpp[1] = {-1};
+}
+#endif
+
+namespace kpp_b200_impl {
+// Species map of the shuffle entries on the device (user index -> KPP index,
+// -1 for user species that take no part in the mechanism).
+__constant__ int c_user_to_kpp[KPP_NUSER > 0 ? KPP_NUSER : 1];
+
+// dir 0: var[kpp[k]][c] = user[k][c]; dir 1: user[k][c] = var[kpp[k]][c].
+// One thread per (cell, user species), cells fastest: both sides coalesced.
+__global__ void shuffle_kernel(int ncells, int nuser, int dir, double* user, long ld_user,
+                               double* var, long ld) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long c = i % ncells, k = i / ncells;
+  if (k >= nuser) return;
+  const int f = c_user_to_kpp[k];
+  if (f < 0) return;
+  if (dir == 0)
+    var[(long)f * ld + c] = user[k * ld_user + c];
+  else
+    user[k * ld_user + c] = var[(long)f * ld + c];
+}
+
+int shuffle(int ncells, double* user, long ld_user, double* var, long ld, int dir,
+            cudaStream_t s) {
+  if (ncells < 0 || ld < ncells || ld_user < ncells) return fail(KPP_B200_EINVAL, "bad sizes");
+  if (ncells == 0 || KPP_NUSER == 0) return KPP_B200_OK;
+  if (!user || !var) return fail(KPP_B200_EINVAL, "null argument");
+  static int uploaded_dev = -1;  // the map is uploaded once per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  if (uploaded_dev != dev) {
+    e = cudaMemcpyToSymbol(c_user_to_kpp, kpp_host::kUserToKpp, sizeof(int) * KPP_NUSER);
+    if (e != cudaSuccess) return cuda_fail("cudaMemcpyToSymbol(species map)", e);
+    uploaded_dev = dev;
+  }
+  const long total = (long)ncells * KPP_NUSER;
+  shuffle_kernel<<<(int)((total + 255) / 256), 256, 0, s>>>(ncells, KPP_NUSER, dir, user,
+                                                              ld_user, var, ld);
+  return check_launch("shuffle_kernel");
+}
+}  // namespace kpp_b200_impl
+
 using namespace kpp_b200_impl;
 
 extern "C" {
+
+int kpp_b200_user_species(int* nuser, int* kpp_index) {
+  if (nuser) *nuser = KPP_NUSER;
+  if (kpp_index)
+    for (int k = 0; k < KPP_NUSER; k++) kpp_index[k] = kpp_host::kUserToKpp[k];
+  return KPP_B200_OK;
+}
+
+int kpp_b200_shuffle_user2kpp(int ncells, int ld_user, const double* v_user, int ld,
+                              double* var, void* stream) {
+  return shuffle(ncells, const_cast<double*>(v_user), ld_user, var, ld, 0, (cudaStream_t)stream);
+}
+
+int kpp_b200_shuffle_kpp2user(int ncells, int ld, const double* var, int ld_user,
+                              double* v_user, void* stream) {
+  return shuffle(ncells, v_user, ld_user, const_cast<double*>(var), ld, 1, (cudaStream_t)stream);
+}
+
 
 int kpp_b200_dims(int* dims) {
   if (!dims) return fail(KPP_B200_EINVAL, "dims is NULL");

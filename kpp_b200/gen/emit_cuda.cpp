@@ -506,6 +506,63 @@ void emit_warp_tables(std::ostream& o, const Mechanism& m) {
 
 }  // namespace
 
+// Host-side files of a mechanism:
+//   <prefix>_host.h        the user-to-KPP species map of the C ABI's
+//                          shuffle entries (GenerateShuffle_user2kpp /
+//                          _kpp2user, src/gen.c:3401-3468): user species k is
+//                          the k-th species declared variable (after #SETFIX)
+//                          among declaration codes 1 .. NSPEC-1, unused ones
+//                          counted, and only k < NVAR are mapped (initNr =
+//                          VarNr, src/kpp.c:594)
+//   <prefix>_Parameters.h  sizes and species indices for a host model in C
+//                          (the generated ROOT_Parameters.h, src/gen.c:2627-2720)
+bool emit_host(const Mechanism& m, const std::string& out_prefix) {
+  View vw(m);
+  const int nvar = m.nvar, nspec = m.nspec;
+  std::vector<int> final_of_slot(m.order.size(), -1);
+  for (int f = 0; f < nspec; f++) final_of_slot[m.spc_slot[f]] = f;
+  // The reference visits declaration codes 1 .. SpcNr-1 only, SpcNr being
+  // the number of species that take part (NSPEC): with unused declared
+  // species the last declarations are never reached.
+  std::vector<int> user;
+  for (int i = 1; i < std::min((int)m.table.size(), nspec); i++) {
+    if (m.table[i].type != SPC_VAR) continue;
+    auto it = m.slot_of_code.find(i);
+    int f = it == m.slot_of_code.end() ? -1 : final_of_slot[it->second];
+    user.push_back(((int)user.size() < nvar && f >= 0) ? f : -1);
+  }
+  {
+    std::ostringstream o;
+    o << "// Generated by kppcu.  Do not edit.  Host data of mechanism " << m.root << ".\n"
+      << "#pragma once\n\n#define KPP_NUSER " << user.size() << "\n\n"
+      << "namespace kpp_host {\n";
+    emit_int_table(o, "kUserToKpp", user);
+    o << "}  // namespace kpp_host\n";
+    std::ofstream f(out_prefix + "_host.h");
+    if (!f) return false;
+    f << o.str();
+  }
+  {
+    std::ostringstream o;
+    o << "/* Generated by kppcu.  Do not edit.  Sizes and species indices of mechanism\n"
+      << "   " << m.root << " (KPP's ROOT_Parameters.h) for host models. */\n"
+      << "#ifndef KPP_B200_" << m.root << "_PARAMETERS_H\n"
+      << "#define KPP_B200_" << m.root << "_PARAMETERS_H\n\n"
+      << "#define NSPEC " << nspec << "\n#define NVAR " << nvar << "\n#define NVARACT "
+      << m.nvaract << "\n#define NFIX " << (m.nfix > 0 ? m.nfix : 1) << "\n#define NREACT "
+      << m.nreact() << "\n#define NVARST 0\n#define NFIXST " << nvar << "\n#define NONZERO "
+      << m.nonzero << "\n#define LU_NONZERO " << m.lu_nonzero << "\n#define CNVAR " << nvar + 1
+      << "\n\n";
+    for (int i = 0; i < nspec; i++) o << "#define ind_" << vw.name(i) << " " << i << "\n";
+    for (int i = nvar; i < nspec; i++) o << "#define indf_" << vw.name(i) << " " << (i - nvar) << "\n";
+    o << "\n#endif\n";
+    std::ofstream f(out_prefix + "_Parameters.h");
+    if (!f) return false;
+    f << o.str();
+  }
+  return true;
+}
+
 bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   View vw(m);
   long ops_fun = 0, ops_jac = 0, ops_decomp = 0, ops_solve = 0;

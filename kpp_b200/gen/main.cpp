@@ -103,7 +103,7 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "kppcu: no variable species\n");
     return 2;
   }
-  if (!emit_cuda(m, out) || !write_json(m, out + ".json")) {
+  if (!emit_cuda(m, out) || !emit_host(m, out) || !write_json(m, out + ".json")) {
     std::fprintf(stderr, "kppcu: cannot write %s\n", out.c_str());
     return 3;
   }

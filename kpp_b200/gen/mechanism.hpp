@@ -78,4 +78,8 @@ void build_structure(Mechanism& m);
 // CUDA emitter: writes <out_prefix>.cuh
 bool emit_cuda(const Mechanism& m, const std::string& out_prefix);
 
+// Host files: <out_prefix>_host.h (species map of the C ABI) and
+// <out_prefix>_Parameters.h (sizes and indices for host models in C).
+bool emit_host(const Mechanism& m, const std::string& out_prefix);
+
 }  // namespace kppcu

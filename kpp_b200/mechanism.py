@@ -94,6 +94,11 @@ class Mechanism:
         L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
         L.kpp_b200_set_kernel.argtypes = [ctypes.c_int]
         L.kpp_b200_set_blocks_per_sm.argtypes = [ctypes.c_int]
+        L.kpp_b200_user_species.argtypes = [_vp, _vp]
+        L.kpp_b200_shuffle_user2kpp.argtypes = [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                _vp, _vp]
+        L.kpp_b200_shuffle_kpp2user.argtypes = [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                _vp, _vp]
         L.kpp_b200_rosenbrock_chain.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int]
             + [_vp] * 2 + [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
@@ -125,6 +130,36 @@ class Mechanism:
         """'auto', 'thread' (one thread per cell) or 'warp' (one warp per cell,
         work set in shared memory); both give bit-identical results."""
         self._check(self.lib.kpp_b200_set_kernel({"auto": 0, "thread": 1, "warp": 2}[which]))
+
+    def user_species(self):
+        """kpp_index[k] of every user species k (declaration order of the
+        variable species; -1: not in the mechanism), as a list."""
+        n = ctypes.c_int()
+        self._check(self.lib.kpp_b200_user_species(ctypes.byref(n), None))
+        idx = (ctypes.c_int * max(n.value, 1))()
+        self._check(self.lib.kpp_b200_user_species(None, idx))
+        return list(idx)[:n.value]
+
+    def shuffle_user2kpp(self, v_user: torch.Tensor, var: torch.Tensor,
+                         stream: Optional[torch.cuda.Stream] = None):
+        """var rows of the mapped user species from v_user ([nuser][ld_user])."""
+        self._dev(v_user, torch.float64, "v_user")
+        self._dev(var, torch.float64, "var")
+        n = var.shape[1]
+        s = stream if stream is not None else torch.cuda.current_stream(var.device)
+        self._check(self.lib.kpp_b200_shuffle_user2kpp(n, v_user.shape[1], _ptr(v_user),
+                                                       var.shape[1], _ptr(var),
+                                                       _vp(s.cuda_stream)))
+
+    def shuffle_kpp2user(self, var: torch.Tensor, v_user: torch.Tensor,
+                         stream: Optional[torch.cuda.Stream] = None):
+        self._dev(v_user, torch.float64, "v_user")
+        self._dev(var, torch.float64, "var")
+        n = var.shape[1]
+        s = stream if stream is not None else torch.cuda.current_stream(var.device)
+        self._check(self.lib.kpp_b200_shuffle_kpp2user(n, var.shape[1], _ptr(var),
+                                                       v_user.shape[1], _ptr(v_user),
+                                                       _vp(s.cuda_stream)))
 
     def set_blocks_per_sm(self, blocks: int):
         """Resident 128-thread blocks per SM of the thread-per-cell launches

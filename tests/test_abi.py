@@ -114,3 +114,30 @@ def test_scheduler_library_exports_every_declared_entry():
         from kpp_b200.scheduler import Mlp, SchedError
         with pytest.raises(SchedError):
             Mlp(10)
+
+
+@pytest.mark.parametrize("mech", MECHS)
+def test_user_species_map_matches_reference_shuffle(mech):
+    """kpp_b200_user_species against the reference's own generated
+    Shuffle_user2kpp / Shuffle_kpp2user (src/gen.c:3401-3468)."""
+    _skip_on_request(mech)
+    from oracle_lib import OracleLib, ensure_built
+    if not ensure_built():
+        pytest.skip("oracle libraries not built")
+    o = OracleLib(mech)
+    idx = Mechanism(mech).user_species()
+    nuser = len(idx)
+    v_user = (np.arange(nuser) + 1.0).astype(np.float64)
+    v = np.full(o.nvar, -1.0)
+    o.lib.Shuffle_user2kpp.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    o.lib.Shuffle_user2kpp(ctypes.c_void_p(v_user.ctypes.data), ctypes.c_void_p(v.ctypes.data))
+    want = np.full(o.nvar, -1.0)
+    for k, f in enumerate(idx):
+        if f >= 0:
+            want[f] = v_user[k]
+    np.testing.assert_array_equal(v, want)
+    back = np.full(nuser, -7.0)
+    o.lib.Shuffle_kpp2user.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    o.lib.Shuffle_kpp2user(ctypes.c_void_p(v.ctypes.data), ctypes.c_void_p(back.ctypes.data))
+    got = np.array([v_user[k] if f >= 0 else -7.0 for k, f in enumerate(idx)])
+    np.testing.assert_array_equal(back, got)

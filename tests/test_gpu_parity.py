@@ -277,3 +277,25 @@ def test_warp_kernel_bit_identical_to_thread_kernel(method, sun_mode):
         m.set_kernel("auto")
     for a, b in zip(*outs):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("mech", MECHS)
+def test_shuffle_entries_follow_the_species_map(mech):
+    m = load(mech)
+    idx = m.user_species()
+    n, nuser = 300, len(idx)
+    vu = torch.rand(nuser, n, dtype=torch.float64, device="cuda")
+    var = torch.full((m.nvar, n), -1.0, dtype=torch.float64, device="cuda")
+    m.shuffle_user2kpp(vu, var)
+    back = torch.full((nuser, n), -7.0, dtype=torch.float64, device="cuda")
+    m.shuffle_kpp2user(var, back)
+    torch.cuda.synchronize()
+    want = np.full((m.nvar, n), -1.0)
+    wback = np.full((nuser, n), -7.0)
+    vu_h = vu.cpu().numpy()
+    for k, f in enumerate(idx):
+        if f >= 0:
+            want[f] = vu_h[k]
+            wback[k] = vu_h[k]
+    np.testing.assert_array_equal(var.cpu().numpy(), want)
+    np.testing.assert_array_equal(back.cpu().numpy(), wback)
