@@ -73,8 +73,20 @@ TRAINING_SUMMARY = {
 # CPU baseline / reference arm (oracle libraries, separate processes)
 # ---------------------------------------------------------------------------
 def _cpu_worker(args):
-    mech, lib_opt, sl_var, sl_fix, temp, cf, sun, t0, t1, atol, rtol, ipar, rpar = args
+    mech, lib_opt, sl_var, sl_fix, temp, cf, sun, t0, t1, atol, rtol, ipar, rpar, sdirk = args
     sys.path.insert(0, str(REPO / "tests"))
+    # the reference integrators print their error messages with printf: keep
+    # them off this pool process's stdout (the bench prints one JSON line)
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    os.close(null)
+    if sdirk is not None:
+        from oracle_lib import SdirkOracle
+        o = SdirkOracle(mech, lib_opt)
+        t = time.perf_counter()
+        o.integrate(sl_var, sl_fix, temp, t0, t1, atol, rtol, sdirk[0], sdirk[1],
+                    cfactor=cf, sun=sun)
+        return time.perf_counter() - t
     from oracle_lib import OracleLib
     o = OracleLib(mech, lib_opt)
     t = time.perf_counter()
@@ -82,9 +94,12 @@ def _cpu_worker(args):
     return time.perf_counter() - t
 
 
-def cpu_reference_rate(wl, ncells_sample: int, procs: int, lib_opt: str = "", pool=None):
+def cpu_reference_rate(wl, ncells_sample: int, procs: int, lib_opt: str = "", pool=None,
+                       sdirk=None):
     """cell-steps/s of the reference C path on `procs` processes, each
-    integrating a contiguous slice of the first `ncells_sample` cells."""
+    integrating a contiguous slice of the first `ncells_sample` cells; with
+    `sdirk` = (ICNTRL, RCNTRL) the reference's SDIRK instead of its
+    Rosenbrock."""
     sub = wl.subset(ncells_sample)
     t0, t1 = sub.step_bounds(0)
     bounds = np.linspace(0, ncells_sample, procs + 1).astype(int)
@@ -95,19 +110,20 @@ def cpu_reference_rate(wl, ncells_sample: int, procs: int, lib_opt: str = "", po
             continue
         sl = slice(a, b)
         opt = lambda x: None if x is None else np.ascontiguousarray(x[sl])
+        fix = sub.fix if sub.fix.shape[0] else np.zeros((1, ncells_sample))  # C pads NFIX
         jobs.append((wl.mech, lib_opt, np.ascontiguousarray(sub.var[:, sl]),
-                     np.ascontiguousarray(sub.fix[:, sl]), sub.temp[sl], opt(sub.cfactor),
-                     opt(sub.sun), t0[sl], t1[sl], sub.atol, sub.rtol, sub.ipar, sub.rpar))
+                     np.ascontiguousarray(fix[:, sl]), sub.temp[sl], opt(sub.cfactor),
+                     opt(sub.sun), t0[sl], t1[sl], sub.atol, sub.rtol, sub.ipar, sub.rpar, sdirk))
     t = time.perf_counter()
     pool.map(_cpu_worker, jobs)
     wall = time.perf_counter() - t
     return ncells_sample / wall, wall
 
 
-def calibrated_sample(wl, procs, pool, target_s=12.0, lib_opt=""):
+def calibrated_sample(wl, procs, pool, target_s=12.0, lib_opt="", sdirk=None):
     """Pick a sample size that takes about target_s of wall time."""
     probe = max(procs * 4, 64)
-    rate, wall = cpu_reference_rate(wl, probe, procs, lib_opt, pool)
+    rate, wall = cpu_reference_rate(wl, probe, procs, lib_opt, pool, sdirk)
     n = int(min(wl.ncells, max(probe, rate * target_s)))
     return n, rate
 
@@ -746,11 +762,175 @@ def run_diurnal(args, rank, world, local_rank):
     }
 
 
+SDIRK_NAMES = {1: "Sdirk2a", 2: "Sdirk2b", 3: "Sdirk3a", 4: "Sdirk4a", 5: "Sdirk4b"}
+
+
+def sdirk_controls(method: int):
+    """ICNTRL / RCNTRL of int/sdirk.c for the workload: scalar tolerances,
+    the given method (0: INTEGRATE's default, Sdirk2a), every other control
+    at its default."""
+    ic, rc = [0] * 20, [0.0] * 20
+    ic[1], ic[2] = 1, method
+    return ic, rc
+
+
+def run_sdirk(args, rank, world, local_rank):
+    """The SDIRK integrator (int/sdirk.c) on the fresh-cell workload: every
+    timed step integrates the same fresh batch over one chemistry step with
+    kpp_b200_sdirk (one launch)."""
+    import torch
+    from kpp_b200 import load, workloads
+    from kpp_b200.build import LIB
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    mech = load(args.mech)
+    wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=shard_seed(rank))
+    n = wl.ncells
+    ic, rc = sdirk_controls(args.sdirk_method)
+    name = SDIRK_NAMES.get(args.sdirk_method, "Sdirk2a")
+    D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    var0 = D(wl.var)
+    var = var0.clone()
+    fix, temp = D(wl.fix), D(wl.temp)
+    cf = D(wl.cfactor) if wl.cfactor is not None else None
+    sun = D(wl.sun) if wl.sun is not None else None
+    atol, rtol = D(wl.atol), D(wl.rtol)
+    t0, t1 = (D(x) for x in wl.step_bounds(0))
+    stream = torch.cuda.current_stream(dev)
+    box = [None]
+
+    def step():
+        var.copy_(var0)  # the same fresh batch every step
+        box[0] = mech.sdirk(var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor=cf, sun=sun,
+                            out=box[0])
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for k in range(args.steps):
+            var.copy_(var0)
+            kev[k][0].record(stream)
+            box[0] = mech.sdirk(var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor=cf, sun=sun,
+                                out=box[0])
+            kev[k][1].record(stream)
+            stats.append(box[0].istatus.sum(dim=1))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        ms = reduce_max(ms, dev)
+    kernel_ms = sum(a.elapsed_time(b) for a, b in kev)
+    ist = torch.stack(stats).sum(dim=0).cpu().numpy().astype(np.int64)
+    nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng = ist.tolist()
+    ierr = box[0].ierr.cpu().numpy()
+    var_dev = var.cpu().numpy()
+
+    # FP64 work from the counters: Fun per Newton iteration, Jac + LU per
+    # factorisation, a solve per Newton iteration and error estimate
+    hdr = REPO / "kpp_b200" / "_gen" / f"{args.mech}.cuh"
+    opsd = {}
+    for line in hdr.read_text().splitlines() if hdr.exists() else []:
+        if line.startswith("#define KPP_OPS_"):
+            _, kk, v = line.split()
+            opsd[kk[8:].lower()] = int(v)
+    flops = (nfun * opsd.get("fun", 0) + njac * opsd.get("jac", 0)
+             + ndec * opsd.get("decomp", 0) + nsol * opsd.get("solve", 0))
+    achieved = flops / (kernel_ms / 1e3) / 1e12
+    peak_fma, _ = fp64_peak(LIB / "libkpp_b200_util.so")
+
+    e2e = None
+    if args.e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        h = {k: pin(v) for k, v in (("var", wl.var), ("fix", wl.fix), ("temp", wl.temp),
+                                    ("t0", wl.step_bounds(0)[0]), ("t1", wl.step_bounds(0)[1]),
+                                    ("atol", wl.atol), ("rtol", wl.rtol))}
+        if wl.cfactor is not None:
+            h["cf"] = pin(wl.cfactor)
+        if wl.sun is not None:
+            h["sun"] = pin(wl.sun)
+        h_out = {"var": torch.empty_like(h["var"]).pin_memory(),
+                 "ist": torch.empty(8, n, dtype=torch.int32).pin_memory(),
+                 "rst": torch.empty(3, n, dtype=torch.float64).pin_memory(),
+                 "ierr": torch.empty(n, dtype=torch.int32).pin_memory()}
+        d = {k: torch.empty_like(v, device=dev) for k, v in h.items()}
+        ebox = [None]
+
+        def e2e_step():
+            for k, v in h.items():
+                d[k].copy_(v, non_blocking=True)
+            ebox[0] = o = mech.sdirk(d["var"], d["fix"], d["temp"], d["t0"], d["t1"], d["atol"],
+                                     d["rtol"], ic, rc, cfactor=d.get("cf"), sun=d.get("sun"),
+                                     out=ebox[0])
+            h_out["var"].copy_(d["var"], non_blocking=True)
+            h_out["ist"].copy_(o.istatus, non_blocking=True)
+            h_out["rst"].copy_(o.rstatus, non_blocking=True)
+            h_out["ierr"].copy_(o.ierr, non_blocking=True)
+            stream.synchronize()
+
+        e2e_step()
+        torch.cuda.synchronize()
+        t_start = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        ems = (time.perf_counter() - t_start) * 1e3
+        if world > 1:
+            ems = reduce_max(ems, dev)
+        nb = lambda x: x.numel() * x.element_size()
+        e2e = {"value": whole_job_rate(n, world, args.steps, ems), "unit": UNIT,
+               "h2d_bytes_per_step": int(sum(nb(v) for v in h.values())),
+               "d2h_bytes_per_step": int(sum(nb(v) for v in h_out.values())),
+               "ms_per_step": ems / args.steps,
+               "api": "Mechanism.sdirk (kpp_b200_sdirk), pinned host arrays copied in and out "
+                      "every step",
+               "matches_device_run": bool(np.array_equal(h_out["var"].numpy(), var_dev))}
+
+    return {
+        "metric": f"{args.mech} cell-steps/s at {n} cells, SDIRK {name} (int/sdirk.c)",
+        "value": whole_job_rate(n, world, args.steps, ms), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{args.mech} {args.workload} (fresh) {name}, {n} cells per GPU, "
+                               f"{wl.dt:.0f} s chemistry step, RTOL {wl.rtol[0]:g} ATOL "
+                               f"{wl.atol[0]:g}, other controls at int/sdirk.c defaults",
+                   "mode": "sdirk", "cells_per_gpu": n, "method": name,
+                   "parallelism": f"cell shards x{world}",
+                   "l2": "inputs larger than L2 (VAR alone %d MB)" % (wl.var.nbytes >> 20)},
+        "impl": "kpp_b200", "gpu_launches": args.steps,
+        "stats": {"internal_steps_per_cell_step": nstp / (n * args.steps),
+                  "rejected_step_rate": nrej / max(nstp, 1),
+                  "ierr_ok_fraction": float((ierr == 1).mean()),
+                  "istatus_sum": dict(zip(["nfun", "njac", "nstp", "nacc", "nrej", "ndec",
+                                           "nsol", "nsng"], map(int, ist)))},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fma, "unit": "TFLOP/s",
+                     "frac": achieved / peak_fma if peak_fma > 0 else None, "traffic": None,
+                     "kernel_ms_per_launch": kernel_ms / args.steps,
+                     "flops_per_cell_step": flops / (n * args.steps),
+                     "peak_source": "measured on this GPU by the DFMA throughput kernel "
+                                    "(kpp_b200/csrc/kpp_util.cu)"},
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }, wl
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal"], default="fresh")
+    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal", "sdirk"], default="fresh")
+    ap.add_argument("--sdirk-method", type=int, default=0,
+                    help="ICNTRL[2] of the SDIRK mode (0: INTEGRATE's default, Sdirk2a)")
     ap.add_argument("--calls", type=int, default=24, help="chemistry steps of a diurnal loop")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["kpp_b200", "reference"], default="kpp_b200")
@@ -778,17 +958,25 @@ def main():
         from kpp_b200 import load, workloads
         mech = load(args.mech)
         wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=workloads.SEED_EVAL)
+        sdirk = sdirk_controls(args.sdirk_method) if args.mode == "sdirk" else None
         with ctx.Pool(procs) as pool:
-            n_sample, _ = calibrated_sample(wl, procs, pool, target_s=min(args.cpu_seconds, 20.0))
+            n_sample, _ = calibrated_sample(wl, procs, pool, target_s=min(args.cpu_seconds, 20.0),
+                                            sdirk=sdirk)
             for _ in range(args.warmup and 1):
-                cpu_reference_rate(wl, max(procs * 4, 64), procs, "", pool)
+                cpu_reference_rate(wl, max(procs * 4, 64), procs, "", pool, sdirk)
             rates, walls = [], []
             for _ in range(args.steps):
-                r, w = cpu_reference_rate(wl, n_sample, procs, "", pool)
+                r, w = cpu_reference_rate(wl, n_sample, procs, "", pool, sdirk)
                 rates.append(r)
                 walls.append(w)
         v = statistics.median(rates)
-        line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        metric = METRIC
+        integ = "int/rosenbrock.c"
+        if sdirk:
+            name = SDIRK_NAMES.get(args.sdirk_method, "Sdirk2a")
+            metric = f"{args.mech} cell-steps/s at {args.ncells} cells, SDIRK {name} (int/sdirk.c)"
+            integ = "int/sdirk.c"
+        line = {"metric": metric, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "impl": "reference",
@@ -797,7 +985,7 @@ def main():
                                        f"{n_sample} of the {args.ncells} cells"},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": "reference",
                                  "sample": f"{n_sample} cells x 1 chemistry step per timed step, "
-                                           f"{procs} processes, KPP-generated C + int/rosenbrock.c "
+                                           f"{procs} processes, KPP-generated C + {integ} "
                                            f"(gcc -O), host CPU {host_cpu_model()}"},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "gpu_launches": 0}
@@ -815,21 +1003,25 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
+    sdirk = sdirk_controls(args.sdirk_method) if args.mode == "sdirk" else None
     if args.mode == "diurnal":
         if pool is not None:
             pool.close()
             pool = None
         result = run_diurnal(args, rank, world, local_rank)
+    elif args.mode == "sdirk":
+        result, wl = run_sdirk(args, rank, world, local_rank)
     else:
         result, wl = run_cuda_arm(args, rank, world, local_rank, pool)
     if pool is not None:
-        n_sample, _ = calibrated_sample(wl, procs, pool, target_s=args.cpu_seconds)
-        rate, wall = cpu_reference_rate(wl, n_sample, procs, "", pool)
+        n_sample, _ = calibrated_sample(wl, procs, pool, target_s=args.cpu_seconds, sdirk=sdirk)
+        rate, wall = cpu_reference_rate(wl, n_sample, procs, "", pool, sdirk)
         pool.close()
+        integ = "int/sdirk.c" if sdirk else "int/rosenbrock.c"
         result["cpu_baseline"] = {
             "value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
             "sample": f"{n_sample} cells x 1 chemistry step of the same workload, {procs} processes "
-                      f"(reference KPP-generated C + int/rosenbrock.c, gcc -O), {wall:.1f} s wall, "
+                      f"(reference KPP-generated C + {integ}, gcc -O), {wall:.1f} s wall, "
                       f"host CPU {host_cpu_model()}"}
     if world > 1:
         import torch.distributed as dist

@@ -98,6 +98,27 @@ int kpp_b200_rosenbrock(int ncells, int ld, double *var, const double *fix,
                         int *istatus, double *rstatus, int *ierr,
                         void *stream);
 
+/* The reference's C SDIRK integrator (int/sdirk.c: SDIRK(N, Tinitial,
+ * Tfinal, Y, RelTol, AbsTol, RCNTRL, ICNTRL, RSTATUS, ISTATUS),
+ * int/sdirk.c:170-511) for every cell, on the same generated Fun / Jac_SP /
+ * LU / solve as the Rosenbrock entries.  icntrl[20] / rcntrl[20] are the C
+ * ICNTRL / RCNTRL: icntrl[1] = 0 vector tolerances, icntrl[2] the method (1
+ * Sdirk2a, 2 Sdirk2b, 3 Sdirk3a, 4 Sdirk4a, 5 Sdirk4b, others Sdirk2a),
+ * icntrl[3] the step limit, icntrl[4] the Newton limit, icntrl[5] = 1 zero
+ * Newton start; rcntrl[0..10] Hmin, Hmax, Hstart, FacMin, FacMax, FacRej,
+ * FacSafe, ThetaMin, NewtonTol, Qmin, Qmax.  Outputs follow the reference's
+ * Fortran-style slots: istatus[8][ld] = ISTATUS[1..8] (Nfun, Njac, Nstp,
+ * Nacc, Nrej, Ndec, Nsol, Nsng of this call), rstatus[3][ld] = RSTATUS[1..3]
+ * (Texit, Hexit, Hnew, set at accepted steps, 0 before), ierr[ld] = the
+ * reference's return value: 1 on success and 0 when it gave up (too many
+ * steps, step too small) -- its error codes are printed, not returned.
+ * Device pointers, asynchronous. */
+int kpp_b200_sdirk(int ncells, int ld, double *var, const double *fix,
+                   const double *temp, const double *cfactor, const double *sun,
+                   const double *tstart, const double *tend, const double *atol,
+                   const double *rtol, const int *icntrl, const double *rcntrl,
+                   int *istatus, double *rstatus, int *ierr, void *stream);
+
 /* The host model's time loop (drv/general.c:59-76) over INTEGRATE
  * (int/rosenbrock.c:94-133) for every cell in one persistent launch: each cell
  * makes ncalls consecutive calls Rosenbrock(T, T + dt) with T = tstart[c]

@@ -23,6 +23,7 @@ import concurrent.futures as cf
 import hashlib
 import json
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -43,10 +44,13 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-diag-suppress", "177"]
 METHOD_PARTS = [1, 2, 3, 4, 5]
+SDIRK_PART = 6  # the SDIRK integrator
 # Mechanisms at or above this LU size keep per-cell work arrays in the
 # cell-fastest global scratch layout instead of thread-local arrays.
 SCRATCH_LU_NONZERO = 200
 
+
+_LINE_MARKER = re.compile(rb"\s*#\s*(line\b|\d)")
 
 def default_kpp_home() -> str:
     home = os.environ.get("KPP_HOME", "")
@@ -164,7 +168,7 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> 
         defines.append("-DKPP_SCRATCH")
     host_header = GEN_OUT / f"{mech}_host.h"
     lib = library_path(mech)
-    parts = [0] + METHOD_PARTS
+    parts = [0] + METHOD_PARTS + [SDIRK_PART]
 
     def part_flags(part: int):
         f = ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT)]
@@ -177,10 +181,11 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> 
         flags = part_flags(part)
         pre = subprocess.run([nvcc(), "-E"] + flags + [str(CSRC / "kpp_rosenbrock.cu")],
                              capture_output=True, check=True).stdout
-        # the code only: line markers and blank lines (comments are already
-        # gone) do not change what is compiled
+        # the code only: line markers (`# 12 "file"`, `#line`) and blank lines
+        # do not change what is compiled (comments are already gone); pragmas
+        # do and are kept
         code = b"\n".join(ln for ln in pre.splitlines()
-                           if ln.strip() and not ln.lstrip().startswith(b"#"))
+                           if ln.strip() and not _LINE_MARKER.match(ln))
         digest = hashlib.sha256(code + " ".join(flags).encode()).hexdigest()
         stamp = objdir / f"part{part}.stamp"
         if not force and obj.exists() and stamp.exists() and stamp.read_text() == digest:

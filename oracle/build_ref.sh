@@ -12,6 +12,8 @@
 #   oracle/_ref/<mech>/libkppref_<mech>.so        -O (reference flags, util/Makefile_c:3)
 #   oracle/_ref/<mech>/libkppref_<mech>_O3.so     -O3 -march=x86-64-v3 (FMA contraction:
 #                                                 the same code with another valid rounding)
+#   oracle/_ref/<mech>_sdirk/libkppsd_<mech>[_O3].so  the model with the reference SDIRK
+#                                                 integrator (int/sdirk.c)
 #
 # The generator is compiled from the unchanged sources in $KPP_REF/src; only
 # the flex/bison front end is replaced by oracle/refkpp/frontend.c because
@@ -95,4 +97,52 @@ EOF
   "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$d" "${srcs[@]}" \
     -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}_O3.so"
   echo "build_ref: $mech -> $d/libkppref_${mech}.so"
+
+  # the same model with the reference SDIRK integrator (int/sdirk.c) and its
+  # batch driver, for the SDIRK entry's parity tests
+  if [ "$mech" != "mcm_isoprene" ]; then
+    ds="$OUT/${mech}_sdirk"
+    rm -rf "$ds"
+    mkdir -p "$ds"
+    cat > "$ds/$mech.kpp" <<EOF
+#MODEL      $mech
+#LANGUAGE   C
+#DOUBLE     ON
+#INTEGRATOR sdirk
+#DRIVER     $HERE/refkpp/batch_driver_sdirk
+#JACOBIAN   SPARSE_LU_ROW
+#HESSIAN    OFF
+#STOICMAT   OFF
+#MEX        OFF
+#INLINE C_GLOBAL
+  extern double kppref_sun_override;
+  extern int kppref_sun_ulps;
+#ENDINLINE
+#INLINE C_RCONST
+  if (kppref_sun_override >= 0.0) SUN = kppref_sun_override;
+  if (kppref_sun_ulps > 0) SUN = nextafter(SUN, 2.0);
+  if (kppref_sun_ulps < 0) SUN = nextafter(SUN, -1.0);
+#ENDINLINE
+EOF
+    (cd "$ds" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
+      echo "build_ref: kpp (sdirk) failed for $mech" >&2; tail -20 "$ds/kpp.log" >&2; exit 1; }
+    srcs=()
+    for f in "$ds/${mech}"_*.c; do
+      case "$f" in *_mex_*) ;; *) srcs+=("$f") ;; esac
+    done
+    "$CC" -O -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm -o "$ds/libkppsd_${mech}.so"
+    "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm \
+      -o "$ds/libkppsd_${mech}_O3.so"
+    # the integrator's pow() calls (step-size factor, Newton tests, SQRT of
+    # the error norm) through the driver's kppsd_pow (refkpp/pow_knob.h),
+    # which can move each result one ulp: another valid rounding of pow
+    others=()
+    for f in "${srcs[@]}"; do
+      case "$f" in *_Integrator.c) ;; *) others+=("$f") ;; esac
+    done
+    "$CC" -O -w -fPIC -c -include "$HERE/refkpp/pow_knob.h" -I"$ds" "$ds/${mech}_Integrator.c" -o "$ds/integrator_pw.o"
+    "$CC" -O -w -fPIC -shared -I"$ds" "${others[@]}" "$ds/integrator_pw.o" -lm \
+      -o "$ds/libkppsd_${mech}_pw.so"
+    echo "build_ref: $mech (sdirk) -> $ds/libkppsd_${mech}.so"
+  fi
 done

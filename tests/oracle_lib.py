@@ -131,3 +131,74 @@ def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, 
         finally:
             o.lib.kppor_set_pow_ulps(ctypes.c_int(0))
     return np.stack(out)
+
+
+def sdirk_lib_path(mech: str, opt: str = "") -> Path:
+    return REF_DIR / f"{mech}_sdirk" / f"libkppsd_{mech}{opt}.so"
+
+
+class SdirkOracle:
+    """The reference's own C SDIRK (int/sdirk.c) on the mechanism's generated
+    model, per cell through oracle/refkpp/batch_driver_sdirk.c."""
+
+    def __init__(self, mech: str, opt: str = ""):
+        self.lib = ctypes.CDLL(str(sdirk_lib_path(mech, opt)))
+        self.lib.kppsd_integrate.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 14
+        d = (ctypes.c_int * 5)()
+        self.lib.kppsd_dims(d)
+        self.nvar = d[0]
+        self.lib.kppsd_set_sun_ulps.argtypes = [ctypes.c_int]
+
+    def set_sun_ulps(self, u: int):
+        self.lib.kppsd_set_sun_ulps(u)
+
+    def set_pow_ulps(self, u: int):
+        """Moves the integrator's pow() results one ulp (the `_pw` build only)."""
+        self.lib.kppsd_set_pow_ulps(ctypes.c_int(u))
+
+    def integrate(self, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl, cfactor=None,
+                  sun=None):
+        """Returns (var_out, istatus [8][n] = ISTATUS[1..8], rstatus [3][n] =
+        RSTATUS[1..3], ierr)."""
+        var = np.ascontiguousarray(var, dtype=np.float64).copy()
+        n = var.shape[1]
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        fix = f64(fix) if fix is not None and np.size(fix) else np.zeros((1, n))
+        temp, tstart, tend, atol, rtol = f64(temp), f64(tstart), f64(tend), f64(atol), f64(rtol)
+        cfactor, sun = f64(cfactor), f64(sun)
+        ic = np.ascontiguousarray(icntrl, dtype=np.int32)
+        rc = np.ascontiguousarray(rcntrl, dtype=np.float64)
+        ist = np.zeros((8, n), np.int32)
+        rst = np.zeros((3, n))
+        ierr = np.zeros(n, np.int32)
+        self.lib.kppsd_integrate(n, n, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun),
+                                 _p(tstart), _p(tend), _p(atol), _p(rtol), _p(ic), _p(rc),
+                                 _p(ist), _p(rst), _p(ierr))
+        return var, ist, rst, ierr
+
+
+def sdirk_alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                     cfactor=None, sun=None):
+    """VAR after the same SDIRK integration by the reference under other
+    valid last-ulp roundings: compiled with FMA contraction; SUN one ulp up
+    and down at every evaluation; the integrator's pow() one ulp up and down
+    (the step-size factor and the Newton convergence tests decide on it)."""
+    out = [SdirkOracle(mech, "_O3").integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl,
+                                              rcntrl, cfactor=cfactor, sun=sun)[0]]
+    o = SdirkOracle(mech)
+    for u in (1, -1):
+        o.set_sun_ulps(u)
+        try:
+            out.append(o.integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                                   cfactor=cfactor, sun=sun)[0])
+        finally:
+            o.set_sun_ulps(0)
+    pw = SdirkOracle(mech, "_pw")
+    for u in (1, -1):
+        pw.set_pow_ulps(u)
+        try:
+            out.append(pw.integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                                    cfactor=cfactor, sun=sun)[0])
+        finally:
+            pw.set_pow_ulps(0)
+    return np.stack(out)
