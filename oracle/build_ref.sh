@@ -96,6 +96,17 @@ EOF
     -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}.so"
   "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$d" "${srcs[@]}" \
     -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}_O3.so"
+  if [ "$mech" != "mcm_isoprene" ]; then
+    # Update_SUN's cos() through the driver's kppref_cos (refkpp/cos_knob.h),
+    # which can move each result one ulp (MCM takes SUN per cell: no cosine)
+    others=()
+    for f in "${srcs[@]}"; do
+      case "$f" in *_Rates.c) ;; *) others+=("$f") ;; esac
+    done
+    "$CC" -O -w -fPIC -c -include "$HERE/refkpp/cos_knob.h" -I"$d" "$d/${mech}_Rates.c" -o "$d/rates_cs.o"
+    "$CC" -O -w -fPIC -shared -I"$d" "${others[@]}" "$d/rates_cs.o" \
+      -x c "$HERE/ros_oracle.c" "${inc[@]}" -lm -o "$d/libkppref_${mech}_cs.so"
+  fi
   echo "build_ref: $mech -> $d/libkppref_${mech}.so"
 
   # the same model with the reference SDIRK integrator (int/sdirk.c) and its
@@ -134,14 +145,16 @@ EOF
     "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm \
       -o "$ds/libkppsd_${mech}_O3.so"
     # the integrator's pow() calls (step-size factor, Newton tests, SQRT of
-    # the error norm) through the driver's kppsd_pow (refkpp/pow_knob.h),
-    # which can move each result one ulp: another valid rounding of pow
+    # the error norm) through the driver's kppsd_pow (refkpp/pow_knob.h), and
+    # Update_SUN's cos() through kppsd_cos (refkpp/cos_knob.h); each can move
+    # its result one ulp: other valid roundings of pow and cos
     others=()
     for f in "${srcs[@]}"; do
-      case "$f" in *_Integrator.c) ;; *) others+=("$f") ;; esac
+      case "$f" in *_Integrator.c|*_Rates.c) ;; *) others+=("$f") ;; esac
     done
     "$CC" -O -w -fPIC -c -include "$HERE/refkpp/pow_knob.h" -I"$ds" "$ds/${mech}_Integrator.c" -o "$ds/integrator_pw.o"
-    "$CC" -O -w -fPIC -shared -I"$ds" "${others[@]}" "$ds/integrator_pw.o" -lm \
+    "$CC" -O -w -fPIC -c -include "$HERE/refkpp/cos_knob.h" -I"$ds" "$ds/${mech}_Rates.c" -o "$ds/rates_pw.o"
+    "$CC" -O -w -fPIC -shared -I"$ds" "${others[@]}" "$ds/integrator_pw.o" "$ds/rates_pw.o" -lm \
       -o "$ds/libkppsd_${mech}_pw.so"
     echo "build_ref: $mech (sdirk) -> $ds/libkppsd_${mech}.so"
   fi

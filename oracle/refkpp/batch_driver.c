@@ -28,6 +28,20 @@ int kppref_sun_ulps = 0;
 /* Test knob: every evaluation moves SUN by one ulp up (1) or down (-1). */
 void kppref_set_sun_ulps(int u) { kppref_sun_ulps = u; }
 
+/* Update_SUN's cos() in the libkppref_<mech>_cs.so build (cos_knob.h
+   force-included into the Rates file): libm's cos, moved one ulp up (1) or
+   down (-1) on request.  Near sunrise and sunset SUN = (1 + cos)/2 cancels,
+   so one ulp of the cosine is a large relative change of SUN there. */
+static int kppref_cos_ulps = 0;
+void kppref_set_cos_ulps(int u) { kppref_cos_ulps = u; }
+double kppref_cos(double x)
+{
+  double r = cos(x);
+  if (kppref_cos_ulps > 0) r = nextafter(r, HUGE_VAL);
+  if (kppref_cos_ulps < 0) r = nextafter(r, -HUGE_VAL);
+  return r;
+}
+
 int Rosenbrock(double Y[], double Tstart, double Tend, double AbsTol[],
                double RelTol[], void (*ode_Fun)(double, double[], double[]),
                void (*ode_Jac)(double, double[], double[]), double RPAR[],

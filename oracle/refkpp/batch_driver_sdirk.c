@@ -38,6 +38,20 @@ double kppsd_pow(double x, double y)
   return r;
 }
 
+/* Update_SUN's cos() in the same build (cos_knob.h force-included into the
+   Rates file): libm's cos, moved one ulp up (1) or down (-1) on request.
+   Near sunrise and sunset SUN = (1 + cos)/2 cancels, so one ulp of the
+   cosine is a large relative change of SUN there. */
+static int kppref_cos_ulps = 0;
+void kppref_set_cos_ulps(int u) { kppref_cos_ulps = u; }
+double kppref_cos(double x)
+{
+  double r = cos(x);
+  if (kppref_cos_ulps > 0) r = nextafter(r, HUGE_VAL);
+  if (kppref_cos_ulps < 0) r = nextafter(r, -HUGE_VAL);
+  return r;
+}
+
 int SDIRK(int N, double Tinitial, double Tfinal, double Y[], double RelTol[],
           double AbsTol[], double RCNTRL[], int ICNTRL[], double RSTATUS[],
           int ISTATUS[]);

@@ -90,6 +90,10 @@ class OracleLib:
         """Move SUN by one ulp up (1) / down (-1) at every evaluation (0: off)."""
         self.lib.kppref_set_sun_ulps(ctypes.c_int(int(u)))
 
+    def set_cos_ulps(self, u: int):
+        """Move Update_SUN's cos() one ulp up (1) / down (-1) (the `_cs` build)."""
+        self.lib.kppref_set_cos_ulps(ctypes.c_int(int(u)))
+
     def fun_jac(self, var, fix, temp, cfactor, sun, t):
         """Rates, Fun and Jac_SP of one cell (1-D var/fix)."""
         var = np.ascontiguousarray(var, dtype=np.float64)
@@ -106,9 +110,12 @@ def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, 
                sun=None, hstart=None):
     """VAR after the same integration by the reference under other valid
     last-ulp roundings: compiled with FMA contraction; SUN moved by one ulp up
-    and down at every evaluation (the size of a cos() difference in
-    Update_SUN); and pow() of the step-size controller one ulp up and down.  Their spread around the reference measures how strongly
-    each entry amplifies last-ulp perturbations."""
+    and down at every evaluation; Update_SUN's cos() one ulp up and down
+    (SUN = (1 + cos)/2 cancels near sunrise and sunset, where a one-ulp
+    cosine moves SUN far more than one ulp of SUN does; built for the
+    mechanisms that compute SUN from TIME); and pow() of the step-size
+    controller one ulp up and down.  Their spread around the reference
+    measures how strongly each entry amplifies last-ulp perturbations."""
     out = []
     o3 = OracleLib(mech, "_O3")
     out.append(o3.integrate(var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, cfactor=cfactor,
@@ -130,6 +137,15 @@ def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, 
                                    cfactor=cfactor, sun=sun, hstart=hstart, which="port")[0])
         finally:
             o.lib.kppor_set_pow_ulps(ctypes.c_int(0))
+    if lib_path(mech, "_cs").exists():
+        cs = OracleLib(mech, "_cs")
+        for u in (1, -1):
+            cs.set_cos_ulps(u)
+            try:
+                out.append(cs.integrate(var, fix, temp, tstart, tend, atol, rtol, ipar, rpar,
+                                        cfactor=cfactor, sun=sun, hstart=hstart)[0])
+            finally:
+                cs.set_cos_ulps(0)
     return np.stack(out)
 
 
@@ -155,6 +171,10 @@ class SdirkOracle:
     def set_pow_ulps(self, u: int):
         """Moves the integrator's pow() results one ulp (the `_pw` build only)."""
         self.lib.kppsd_set_pow_ulps(ctypes.c_int(u))
+
+    def set_cos_ulps(self, u: int):
+        """Moves Update_SUN's cos() results one ulp (the `_pw` build only)."""
+        self.lib.kppref_set_cos_ulps(ctypes.c_int(u))
 
     def integrate(self, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl, cfactor=None,
                   sun=None):
@@ -182,7 +202,10 @@ def sdirk_alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, icntrl
     """VAR after the same SDIRK integration by the reference under other
     valid last-ulp roundings: compiled with FMA contraction; SUN one ulp up
     and down at every evaluation; the integrator's pow() one ulp up and down
-    (the step-size factor and the Newton convergence tests decide on it)."""
+    (the step-size factor and the Newton convergence tests decide on it);
+    Update_SUN's cos() one ulp up and down (SUN = (1 + cos)/2 cancels near
+    sunrise and sunset, where a one-ulp cosine moves SUN far more than one
+    ulp of SUN does)."""
     out = [SdirkOracle(mech, "_O3").integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl,
                                               rcntrl, cfactor=cfactor, sun=sun)[0]]
     o = SdirkOracle(mech)
@@ -194,11 +217,12 @@ def sdirk_alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, icntrl
         finally:
             o.set_sun_ulps(0)
     pw = SdirkOracle(mech, "_pw")
-    for u in (1, -1):
-        pw.set_pow_ulps(u)
-        try:
-            out.append(pw.integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
-                                    cfactor=cfactor, sun=sun)[0])
-        finally:
-            pw.set_pow_ulps(0)
+    for knob in (pw.set_pow_ulps, pw.set_cos_ulps):
+        for u in (1, -1):
+            knob(u)
+            try:
+                out.append(pw.integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                                        cfactor=cfactor, sun=sun)[0])
+            finally:
+                knob(0)
     return np.stack(out)

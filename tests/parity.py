@@ -12,9 +12,11 @@ perturbations far beyond 1e-9: small_strato's atomic oxygen at night
 (~1e-15 molec/cm3) is the difference of nearly equal stage terms, and the
 reference itself, compiled with FMA contraction (another valid rounding of
 the same code, oracle/_ref/*/libkppref_*_O3.so), moves by ~1e-6 there.  The
-reference's own spread is measured with five alternates (FMA contraction;
-SUN one ulp up and down at every evaluation; pow() of the step-size
-controller one ulp up and down; oracle_lib.alternates).  Every
+reference's own spread is measured with alternates (FMA contraction;
+SUN one ulp up and down at every evaluation; Update_SUN's cosine one ulp up
+and down, which near sunrise and sunset moves SUN far more than one ulp of
+SUN; pow() of the integrator one ulp up and down; oracle_lib.alternates and
+oracle_lib.sdirk_alternates).  Every
 entry above FLOOR must be within REL_TOL of the reference, or, where the
 reference does not reproduce itself to REL_TOL, within ILL_FACTOR times the
 reference's own spread (the alternates sample that spread, so the factor

@@ -131,3 +131,47 @@ def test_restatement_reproduces_golden_vectors(mech, golden_dir):
         np.testing.assert_array_equal(var, g["var"][k])
         np.testing.assert_array_equal(ist, g["istatus"][k])
         np.testing.assert_array_equal(ierr, g["ierr"][k])
+
+
+@pytest.mark.parametrize("mech", ["small_strato", "saprc99"])
+def test_rounding_alternate_builds_reproduce_reference_with_knobs_off(mech):
+    """The builds behind the parity bar's rounding alternates (the reference
+    with Update_SUN's cos(), or the SDIRK integrator's pow() and cos(),
+    routed through a one-ulp knob) are the reference itself with the knob
+    off, and move results with it on."""
+    from oracle_lib import SdirkOracle, lib_path, sdirk_lib_path
+    if not (lib_path(mech, "_cs").exists() and sdirk_lib_path(mech, "_pw").exists()):
+        pytest.skip("rounding-alternate builds not present")
+    o = OracleLib(mech)
+    n = 64
+    wl = workloads.for_mechanism(_View(o), mech, n, seed=17)
+    fix = wl.fix if wl.fix.shape[0] else np.zeros((1, n))
+    # a window across sunrise or sunset, where the cosine matters
+    t0, t1 = wl.step_bounds(3)
+    kw = dict(cfactor=wl.cfactor, sun=None)  # SUN from TIME: Update_SUN runs
+    cs = OracleLib(mech, "_cs")
+    ref = o.integrate(wl.var, fix, wl.temp, t0, t1, wl.atol, wl.rtol, wl.ipar, wl.rpar, **kw)
+    got = cs.integrate(wl.var, fix, wl.temp, t0, t1, wl.atol, wl.rtol, wl.ipar, wl.rpar, **kw)
+    for a, b in zip(ref, got):
+        np.testing.assert_array_equal(a, b)
+    cs.set_cos_ulps(1)
+    try:
+        moved = cs.integrate(wl.var, fix, wl.temp, t0, t1, wl.atol, wl.rtol, wl.ipar, wl.rpar, **kw)
+    finally:
+        cs.set_cos_ulps(0)
+    assert not np.array_equal(moved[0], ref[0])
+
+    ic, rc = [0] * 20, [0.0] * 20
+    ic[1], ic[2] = 1, 3
+    sd, pw = SdirkOracle(mech), SdirkOracle(mech, "_pw")
+    ref = sd.integrate(wl.var, fix, wl.temp, t0, t1, wl.atol, wl.rtol, ic, rc, **kw)
+    got = pw.integrate(wl.var, fix, wl.temp, t0, t1, wl.atol, wl.rtol, ic, rc, **kw)
+    for a, b in zip(ref, got):
+        np.testing.assert_array_equal(a, b)
+    for knob in (pw.set_pow_ulps, pw.set_cos_ulps):
+        knob(-1)
+        try:
+            moved = pw.integrate(wl.var, fix, wl.temp, t0, t1, wl.atol, wl.rtol, ic, rc, **kw)
+        finally:
+            knob(0)
+        assert not np.array_equal(moved[0], ref[0])
