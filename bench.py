@@ -73,18 +73,18 @@ TRAINING_SUMMARY = {
 # CPU baseline / reference arm (oracle libraries, separate processes)
 # ---------------------------------------------------------------------------
 def _cpu_worker(args):
-    mech, lib_opt, sl_var, sl_fix, temp, cf, sun, t0, t1, atol, rtol, ipar, rpar, sdirk = args
+    mech, lib_opt, sl_var, sl_fix, temp, cf, sun, t0, t1, atol, rtol, ipar, rpar, integ = args
     sys.path.insert(0, str(REPO / "tests"))
     # the reference integrators print their error messages with printf: keep
     # them off this pool process's stdout (the bench prints one JSON line)
     null = os.open(os.devnull, os.O_WRONLY)
     os.dup2(null, 1)
     os.close(null)
-    if sdirk is not None:
-        from oracle_lib import SdirkOracle
-        o = SdirkOracle(mech, lib_opt)
+    if integ is not None:
+        from oracle_lib import RkOracle, SdirkOracle
+        o = (SdirkOracle if integ[0] == "sdirk" else RkOracle)(mech, lib_opt)
         t = time.perf_counter()
-        o.integrate(sl_var, sl_fix, temp, t0, t1, atol, rtol, sdirk[0], sdirk[1],
+        o.integrate(sl_var, sl_fix, temp, t0, t1, atol, rtol, integ[1], integ[2],
                     cfactor=cf, sun=sun)
         return time.perf_counter() - t
     from oracle_lib import OracleLib
@@ -95,11 +95,11 @@ def _cpu_worker(args):
 
 
 def cpu_reference_rate(wl, ncells_sample: int, procs: int, lib_opt: str = "", pool=None,
-                       sdirk=None):
+                       integ=None):
     """cell-steps/s of the reference C path on `procs` processes, each
     integrating a contiguous slice of the first `ncells_sample` cells; with
-    `sdirk` = (ICNTRL, RCNTRL) the reference's SDIRK instead of its
-    Rosenbrock."""
+    `integ` = (kind, ICNTRL, RCNTRL) the reference's SDIRK ("sdirk") or
+    Runge-Kutta ("rk") integrator instead of its Rosenbrock."""
     sub = wl.subset(ncells_sample)
     t0, t1 = sub.step_bounds(0)
     bounds = np.linspace(0, ncells_sample, procs + 1).astype(int)
@@ -113,17 +113,17 @@ def cpu_reference_rate(wl, ncells_sample: int, procs: int, lib_opt: str = "", po
         fix = sub.fix if sub.fix.shape[0] else np.zeros((1, ncells_sample))  # C pads NFIX
         jobs.append((wl.mech, lib_opt, np.ascontiguousarray(sub.var[:, sl]),
                      np.ascontiguousarray(fix[:, sl]), sub.temp[sl], opt(sub.cfactor),
-                     opt(sub.sun), t0[sl], t1[sl], sub.atol, sub.rtol, sub.ipar, sub.rpar, sdirk))
+                     opt(sub.sun), t0[sl], t1[sl], sub.atol, sub.rtol, sub.ipar, sub.rpar, integ))
     t = time.perf_counter()
     pool.map(_cpu_worker, jobs)
     wall = time.perf_counter() - t
     return ncells_sample / wall, wall
 
 
-def calibrated_sample(wl, procs, pool, target_s=12.0, lib_opt="", sdirk=None):
+def calibrated_sample(wl, procs, pool, target_s=12.0, lib_opt="", integ=None):
     """Pick a sample size that takes about target_s of wall time."""
     probe = max(procs * 4, 64)
-    rate, wall = cpu_reference_rate(wl, probe, procs, lib_opt, pool, sdirk)
+    rate, wall = cpu_reference_rate(wl, probe, procs, lib_opt, pool, integ)
     n = int(min(wl.ncells, max(probe, rate * target_s)))
     return n, rate
 
@@ -763,21 +763,43 @@ def run_diurnal(args, rank, world, local_rank):
 
 
 SDIRK_NAMES = {1: "Sdirk2a", 2: "Sdirk2b", 3: "Sdirk3a", 4: "Sdirk4a", 5: "Sdirk4b"}
+RK_NAMES = {0: "Radau-2A", 1: "Radau-2A", 2: "Lobatto-3C", 3: "Gauss", 4: "Radau-1A",
+            5: "Lobatto-3A"}
+# kind: (entry of kpp_b200.Mechanism, reference file, method names, default name)
+INTEGRATORS = {"sdirk": ("sdirk", "int/sdirk.c", SDIRK_NAMES, "Sdirk2a"),
+               "rk": ("runge_kutta", "int/runge_kutta.c", RK_NAMES, "Radau-2A")}
 
 
-def sdirk_controls(method: int):
-    """ICNTRL / RCNTRL of int/sdirk.c for the workload: scalar tolerances,
-    the given method (0: INTEGRATE's default, Sdirk2a), every other control
-    at its default."""
+def integrator_controls(kind: str, method: int):
+    """(kind, ICNTRL, RCNTRL) for the workload's scalar tolerances and the
+    given method, every other control at its default; for Runge-Kutta with
+    INTEGRATE's SDIRK error estimator (int/runge_kutta.c:131-139)."""
     ic, rc = [0] * 20, [0.0] * 20
     ic[1], ic[2] = 1, method
-    return ic, rc
+    if kind == "rk":
+        ic[9] = 1
+    return kind, ic, rc
 
 
-def run_sdirk(args, rank, world, local_rank):
-    """The SDIRK integrator (int/sdirk.c) on the fresh-cell workload: every
-    timed step integrates the same fresh batch over one chemistry step with
-    kpp_b200_sdirk (one launch)."""
+def mode_integrator(args):
+    """(kind, ICNTRL, RCNTRL) of the --mode sdirk / rk runs, else None."""
+    if args.mode == "sdirk":
+        return integrator_controls("sdirk", args.sdirk_method)
+    if args.mode == "rk":
+        return integrator_controls("rk", args.rk_method)
+    return None
+
+
+def integrator_name(kind: str, method: int) -> str:
+    names, default = INTEGRATORS[kind][2], INTEGRATORS[kind][3]
+    return names.get(method, default)
+
+
+def run_integrator(args, rank, world, local_rank, kind: str):
+    """The SDIRK (int/sdirk.c) or Runge-Kutta (int/runge_kutta.c)
+    integrator on the fresh-cell workload: every timed step integrates the
+    same fresh batch over one chemistry step with kpp_b200_sdirk /
+    kpp_b200_runge_kutta (one launch)."""
     import torch
     from kpp_b200 import load, workloads
     from kpp_b200.build import LIB
@@ -787,8 +809,11 @@ def run_sdirk(args, rank, world, local_rank):
     mech = load(args.mech)
     wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=shard_seed(rank))
     n = wl.ncells
-    ic, rc = sdirk_controls(args.sdirk_method)
-    name = SDIRK_NAMES.get(args.sdirk_method, "Sdirk2a")
+    method = args.sdirk_method if kind == "sdirk" else args.rk_method
+    _, ic, rc = integrator_controls(kind, method)
+    name = integrator_name(kind, method)
+    entry_name, source = INTEGRATORS[kind][0], INTEGRATORS[kind][1]
+    entry = getattr(mech, entry_name)
     D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     var0 = D(wl.var)
     var = var0.clone()
@@ -802,7 +827,7 @@ def run_sdirk(args, rank, world, local_rank):
 
     def step():
         var.copy_(var0)  # the same fresh batch every step
-        box[0] = mech.sdirk(var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor=cf, sun=sun,
+        box[0] = entry(var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor=cf, sun=sun,
                             out=box[0])
 
     for _ in range(args.warmup):
@@ -821,7 +846,7 @@ def run_sdirk(args, rank, world, local_rank):
         for k in range(args.steps):
             var.copy_(var0)
             kev[k][0].record(stream)
-            box[0] = mech.sdirk(var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor=cf, sun=sun,
+            box[0] = entry(var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor=cf, sun=sun,
                                 out=box[0])
             kev[k][1].record(stream)
             stats.append(box[0].istatus.sum(dim=1))
@@ -836,16 +861,27 @@ def run_sdirk(args, rank, world, local_rank):
     ierr = box[0].ierr.cpu().numpy()
     var_dev = var.cpu().numpy()
 
-    # FP64 work from the counters: Fun per Newton iteration, Jac + LU per
-    # factorisation, a solve per Newton iteration and error estimate
-    hdr = REPO / "kpp_b200" / "_gen" / f"{args.mech}.cuh"
+    # FP64 work from the counters.  SDIRK: Fun per Newton iteration, Jac +
+    # LU per factorisation, a solve per Newton iteration and error estimate.
+    # Runge-Kutta (a lower bound: the SDIRK estimator's solves and the
+    # estimator's extra Fun calls that ISTATUS does not count are left out):
+    # the counted Fun calls plus three stage evaluations per Newton iteration
+    # (one RK_Solve each), a real and a complex LU per factorisation, a real
+    # and a complex solve per Newton iteration.
     opsd = {}
-    for line in hdr.read_text().splitlines() if hdr.exists() else []:
-        if line.startswith("#define KPP_OPS_"):
-            _, kk, v = line.split()
-            opsd[kk[8:].lower()] = int(v)
-    flops = (nfun * opsd.get("fun", 0) + njac * opsd.get("jac", 0)
-             + ndec * opsd.get("decomp", 0) + nsol * opsd.get("solve", 0))
+    for hname in (f"{args.mech}.cuh", f"{args.mech}_cmplx.cuh"):
+        hdr = REPO / "kpp_b200" / "_gen" / hname
+        for line in hdr.read_text().splitlines() if hdr.exists() else []:
+            if line.startswith("#define KPP_OPS_"):
+                _, kk, v = line.split()
+                opsd[kk[8:].lower()] = int(v)
+    if kind == "sdirk":
+        flops = (nfun * opsd.get("fun", 0) + njac * opsd.get("jac", 0)
+                 + ndec * opsd.get("decomp", 0) + nsol * opsd.get("solve", 0))
+    else:
+        flops = ((nfun + 3 * nsol) * opsd.get("fun", 0) + njac * opsd.get("jac", 0)
+                 + ndec * (opsd.get("decomp", 0) + opsd.get("decomp_cmplx", 0))
+                 + nsol * (opsd.get("solve", 0) + opsd.get("solve_cmplx", 0)))
     achieved = flops / (kernel_ms / 1e3) / 1e12
     peak_fma, _ = fp64_peak(LIB / "libkpp_b200_util.so")
 
@@ -869,7 +905,7 @@ def run_sdirk(args, rank, world, local_rank):
         def e2e_step():
             for k, v in h.items():
                 d[k].copy_(v, non_blocking=True)
-            ebox[0] = o = mech.sdirk(d["var"], d["fix"], d["temp"], d["t0"], d["t1"], d["atol"],
+            ebox[0] = o = entry(d["var"], d["fix"], d["temp"], d["t0"], d["t1"], d["atol"],
                                      d["rtol"], ic, rc, cfactor=d.get("cf"), sun=d.get("sun"),
                                      out=ebox[0])
             h_out["var"].copy_(d["var"], non_blocking=True)
@@ -891,20 +927,20 @@ def run_sdirk(args, rank, world, local_rank):
                "h2d_bytes_per_step": int(sum(nb(v) for v in h.values())),
                "d2h_bytes_per_step": int(sum(nb(v) for v in h_out.values())),
                "ms_per_step": ems / args.steps,
-               "api": "Mechanism.sdirk (kpp_b200_sdirk), pinned host arrays copied in and out "
-                      "every step",
+               "api": f"Mechanism.{entry_name} (kpp_b200_{entry_name}), pinned host arrays "
+                      "copied in and out every step",
                "matches_device_run": bool(np.array_equal(h_out["var"].numpy(), var_dev))}
 
     return {
-        "metric": f"{args.mech} cell-steps/s at {n} cells, SDIRK {name} (int/sdirk.c)",
+        "metric": f"{args.mech} cell-steps/s at {n} cells, {kind.upper()} {name} ({source})",
         "value": whole_job_rate(n, world, args.steps, ms), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"{args.mech} {args.workload} (fresh) {name}, {n} cells per GPU, "
                                f"{wl.dt:.0f} s chemistry step, RTOL {wl.rtol[0]:g} ATOL "
-                               f"{wl.atol[0]:g}, other controls at int/sdirk.c defaults",
-                   "mode": "sdirk", "cells_per_gpu": n, "method": name,
+                               f"{wl.atol[0]:g}, other controls at {source} defaults",
+                   "mode": kind, "cells_per_gpu": n, "method": name,
                    "parallelism": f"cell shards x{world}",
                    "l2": "inputs larger than L2 (VAR alone %d MB)" % (wl.var.nbytes >> 20)},
         "impl": "kpp_b200", "gpu_launches": args.steps,
@@ -928,9 +964,12 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal", "sdirk"], default="fresh")
+    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal", "sdirk", "rk"],
+                    default="fresh")
     ap.add_argument("--sdirk-method", type=int, default=0,
                     help="ICNTRL[2] of the SDIRK mode (0: INTEGRATE's default, Sdirk2a)")
+    ap.add_argument("--rk-method", type=int, default=0,
+                    help="ICNTRL[2] of the Runge-Kutta mode (0: INTEGRATE's default, Radau-2A)")
     ap.add_argument("--calls", type=int, default=24, help="chemistry steps of a diurnal loop")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["kpp_b200", "reference"], default="kpp_b200")
@@ -958,24 +997,26 @@ def main():
         from kpp_b200 import load, workloads
         mech = load(args.mech)
         wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=workloads.SEED_EVAL)
-        sdirk = sdirk_controls(args.sdirk_method) if args.mode == "sdirk" else None
+        integ = mode_integrator(args)
         with ctx.Pool(procs) as pool:
             n_sample, _ = calibrated_sample(wl, procs, pool, target_s=min(args.cpu_seconds, 20.0),
-                                            sdirk=sdirk)
+                                            integ=integ)
             for _ in range(args.warmup and 1):
-                cpu_reference_rate(wl, max(procs * 4, 64), procs, "", pool, sdirk)
+                cpu_reference_rate(wl, max(procs * 4, 64), procs, "", pool, integ)
             rates, walls = [], []
             for _ in range(args.steps):
-                r, w = cpu_reference_rate(wl, n_sample, procs, "", pool, sdirk)
+                r, w = cpu_reference_rate(wl, n_sample, procs, "", pool, integ)
                 rates.append(r)
                 walls.append(w)
         v = statistics.median(rates)
         metric = METRIC
-        integ = "int/rosenbrock.c"
-        if sdirk:
-            name = SDIRK_NAMES.get(args.sdirk_method, "Sdirk2a")
-            metric = f"{args.mech} cell-steps/s at {args.ncells} cells, SDIRK {name} (int/sdirk.c)"
-            integ = "int/sdirk.c"
+        source = "int/rosenbrock.c"
+        if integ:
+            kind = integ[0]
+            source = INTEGRATORS[kind][1]
+            name = integrator_name(kind, integ[1][2])
+            metric = (f"{args.mech} cell-steps/s at {args.ncells} cells, {kind.upper()} {name} "
+                      f"({source})")
         line = {"metric": metric, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -985,7 +1026,7 @@ def main():
                                        f"{n_sample} of the {args.ncells} cells"},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": "reference",
                                  "sample": f"{n_sample} cells x 1 chemistry step per timed step, "
-                                           f"{procs} processes, KPP-generated C + {integ} "
+                                           f"{procs} processes, KPP-generated C + {source} "
                                            f"(gcc -O), host CPU {host_cpu_model()}"},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "gpu_launches": 0}
@@ -1003,25 +1044,25 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    sdirk = sdirk_controls(args.sdirk_method) if args.mode == "sdirk" else None
+    integ = mode_integrator(args)
     if args.mode == "diurnal":
         if pool is not None:
             pool.close()
             pool = None
         result = run_diurnal(args, rank, world, local_rank)
-    elif args.mode == "sdirk":
-        result, wl = run_sdirk(args, rank, world, local_rank)
+    elif integ is not None:
+        result, wl = run_integrator(args, rank, world, local_rank, integ[0])
     else:
         result, wl = run_cuda_arm(args, rank, world, local_rank, pool)
     if pool is not None:
-        n_sample, _ = calibrated_sample(wl, procs, pool, target_s=args.cpu_seconds, sdirk=sdirk)
-        rate, wall = cpu_reference_rate(wl, n_sample, procs, "", pool, sdirk)
+        n_sample, _ = calibrated_sample(wl, procs, pool, target_s=args.cpu_seconds, integ=integ)
+        rate, wall = cpu_reference_rate(wl, n_sample, procs, "", pool, integ)
         pool.close()
-        integ = "int/sdirk.c" if sdirk else "int/rosenbrock.c"
+        source = INTEGRATORS[integ[0]][1] if integ else "int/rosenbrock.c"
         result["cpu_baseline"] = {
             "value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
             "sample": f"{n_sample} cells x 1 chemistry step of the same workload, {procs} processes "
-                      f"(reference KPP-generated C + {integ}, gcc -O), {wall:.1f} s wall, "
+                      f"(reference KPP-generated C + {source}, gcc -O), {wall:.1f} s wall, "
                       f"host CPU {host_cpu_model()}"}
     if world > 1:
         import torch.distributed as dist

@@ -119,6 +119,31 @@ int kpp_b200_sdirk(int ncells, int ld, double *var, const double *fix,
                    const double *rtol, const int *icntrl, const double *rcntrl,
                    int *istatus, double *rstatus, int *ierr, void *stream);
 
+/* The reference's C fully implicit Runge-Kutta integrator (int/runge_kutta.c:
+ * RungeKutta(N, T, Tend, Y, RelTol, AbsTol, RCNTRL, ICNTRL, RSTATUS, ISTATUS,
+ * &IERR), int/runge_kutta.c:203-1001) for every cell, with the complex LU of
+ * util/sutil.c:28-90 generated for the mechanism.  icntrl[20] / rcntrl[20]
+ * are the C ICNTRL / RCNTRL: icntrl[1] = 0 vector tolerances, icntrl[2] the
+ * method (0 or 1 Radau-2A, 2 Lobatto-3C, 3 Gauss, 4 Radau-1A, 5 Lobatto-3A),
+ * icntrl[3] the step limit, icntrl[4] the Newton limit, icntrl[5] = 1 zero
+ * Newton start, icntrl[9] = 1 the SDIRK error estimator (0 the classic one),
+ * icntrl[10] = 1 the classic step controller (0 Gustafsson's);
+ * rcntrl[0..10] Hmin, Hmax, Hstart, FacMin, FacMax, FacRej, FacSafe,
+ * ThetaMin, NewtonTol, Qmin, Qmax.  Outputs: istatus[8][ld] = ISTATUS[0..7]
+ * (Nfun, Njac, Nstp, Nacc, Nrej, Ndec, Nsol, Nsng, counted as the reference
+ * counts them), rstatus[3][ld] = RSTATUS[0..2] (Texit, Hacc, Hnew), ierr[ld]
+ * = IERR: 1, or the last failing parameter check (-1, -2, -4 .. -8, -13) with
+ * no step taken.  The reference prints the errors it meets while integrating
+ * and carries on; here a cell whose step size becomes 0 or NaN stops with
+ * -10 and one that needs more than icntrl[3] + 200000 steps with -9 (the
+ * reference would not return from either).  Mechanisms with LU_NONZERO <
+ * 2000 only (KPP_B200_EINVAL otherwise).  Device pointers, asynchronous. */
+int kpp_b200_runge_kutta(int ncells, int ld, double *var, const double *fix,
+                         const double *temp, const double *cfactor, const double *sun,
+                         const double *tstart, const double *tend, const double *atol,
+                         const double *rtol, const int *icntrl, const double *rcntrl,
+                         int *istatus, double *rstatus, int *ierr, void *stream);
+
 /* The host model's time loop (drv/general.c:59-76) over INTEGRATE
  * (int/rosenbrock.c:94-133) for every cell in one persistent launch: each cell
  * makes ncalls consecutive calls Rosenbrock(T, T + dt) with T = tstart[c]

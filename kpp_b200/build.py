@@ -45,6 +45,7 @@ NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-
               "-diag-suppress", "177"]
 METHOD_PARTS = [1, 2, 3, 4, 5]
 SDIRK_PART = 6  # the SDIRK integrator
+RK_PART = 7     # the Runge-Kutta integrator (complex LU from <mech>_cmplx.cuh)
 # Mechanisms at or above this LU size keep per-cell work arrays in the
 # cell-fastest global scratch layout instead of thread-local arrays.
 SCRATCH_LU_NONZERO = 200
@@ -155,8 +156,8 @@ def library_path(mech: str) -> Path:
 
 
 def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> Path:
-    """nvcc each part (the C ABI, one part per Rosenbrock method) in parallel
-    and link the shared library.  A part is recompiled only when its own
+    """nvcc each part (the C ABI, one part per Rosenbrock method, the SDIRK
+    and the Runge-Kutta integrators) in parallel and link the shared library.  A part is recompiled only when its own
     preprocessed source or flags change (large mechanisms take many minutes
     per part), so a change confined to the C ABI rebuilds part 0 alone."""
     LIB.mkdir(exist_ok=True)
@@ -168,12 +169,14 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> 
         defines.append("-DKPP_SCRATCH")
     host_header = GEN_OUT / f"{mech}_host.h"
     lib = library_path(mech)
-    parts = [0] + METHOD_PARTS + [SDIRK_PART]
+    parts = [0] + METHOD_PARTS + [SDIRK_PART, RK_PART]
 
     def part_flags(part: int):
         f = ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT)]
         if part == 0 and host_header.exists():
             f.append(f'-DKPP_HOST_HEADER="{host_header}"')
+        if part == RK_PART:
+            f.append(f'-DKPP_CMPLX_HEADER="{header.with_name(header.stem + "_cmplx.cuh")}"')
         return f
 
     def compile_part(part: int):

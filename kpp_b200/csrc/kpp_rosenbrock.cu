@@ -32,6 +32,9 @@
 #include "../../include/kpp_b200.h"
 #include "kpp_ratelaws.cuh"
 #include KPP_MECH_HEADER
+#if KPP_PART == 7 && KPP_LU_NONZERO < 2000
+#include KPP_CMPLX_HEADER
+#endif
 
 // Translation-unit split (the build compiles this file once per part, in
 // parallel): KPP_PART 1..5 holds the kernel of Rosenbrock method 1..5 and its
@@ -502,7 +505,63 @@ int launch_sdirk(LaunchArgs& a, int grid, cudaStream_t s) {
 }
 #endif  // KPP_PART == 6
 
+#if KPP_PART == 7
+#include "kpp_rk.cuh"
+
+#if KPP_LU_NONZERO < 2000
+// One thread slot integrates cells slot, slot + nslots, ... with the C
+// RungeKutta (int/runge_kutta.c); the shared controls and the method table
+// come in `c`, RCNTRL in rpar of the launch.
+__global__ void
+#if KPP_MIN_BLOCKS > 0
+__launch_bounds__(128, KPP_MIN_BLOCKS)
+#else
+__launch_bounds__(128)
+#endif
+rk_kernel(const LaunchArgs a, const rk::Controls c) {
+  const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long ld = a.ld;
+  rk::Work w(a.scratch, slot);
+  for (long cc = slot; cc < a.ncells; cc += a.nslots) {
+    const int cell = (int)cc;
+    CellEnv env;
+    load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
+#pragma unroll 4
+    for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
+    Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
+    double rst[3] = {0.0, 0.0, 0.0};
+    const int ierr =
+        rk::rk_cell(env, w, c, a.tstart[cell], a.tend[cell], a.rpar, a.atol, a.rtol, rst, st);
+    a.ierr[cell] = ierr;
+#pragma unroll 4
+    for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+    const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
+#pragma unroll
+    for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
+#pragma unroll
+    for (int i = 0; i < 3; i++) a.rstatus[i * ld + cell] = rst[i];
+  }
+}
+
+int launch_rk(LaunchArgs& a, int grid, cudaStream_t s) {
+  const rk::Controls c = rk::make_controls(a.ipar, a.rpar);
+  rk_kernel<<<grid, kBlock, 0, s>>>(a, c);
+  return check_launch("rk_kernel");
+}
+#else
+int launch_rk(LaunchArgs&, int, cudaStream_t) {
+  return fail(KPP_B200_EINVAL,
+              "kpp_b200_runge_kutta: built for mechanisms with LU_NONZERO < 2000 only");
+}
+#endif
+#endif  // KPP_PART == 7
+
 #else  // KPP_PART == 0
+
+#define KPP_RK_HOST_ONLY
+#include "kpp_rk.cuh"
+// The Runge-Kutta kernel (KPP_PART 7).
+int launch_rk(LaunchArgs& a, int grid, cudaStream_t s);
 
 thread_local char g_last_error[512] = "";
 
@@ -1102,6 +1161,25 @@ int kpp_b200_sdirk(int ncells, int ld, double* var, const double* fix, const dou
   if (rc != KPP_B200_OK) return rc;
   a.scratch_doubles = bytes / sizeof(double);
   return launch_sdirk(a, (int)(a.nslots / kBlock), s);
+}
+
+int kpp_b200_runge_kutta(int ncells, int ld, double* var, const double* fix,
+                         const double* temp, const double* cfactor, const double* sun,
+                         const double* tstart, const double* tend, const double* atol,
+                         const double* rtol, const int* icntrl, const double* rcntrl,
+                         int* istatus, double* rstatus, int* ierr, void* stream) {
+  LaunchArgs a;
+  int rc = fill_args(a, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol,
+                     icntrl, rcntrl, nullptr, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  a.nslots = slots_for(ncells);
+  const size_t bytes = kUsesScratch ? (size_t)kRkPerSlot * (size_t)kSlotStride * sizeof(double)
+                                    : 0;
+  rc = cached_scratch(s, bytes, &a.scratch);
+  if (rc != KPP_B200_OK) return rc;
+  a.scratch_doubles = bytes / sizeof(double);
+  return launch_rk(a, (int)(a.nslots / kBlock), s);
 }
 
 int kpp_b200_rosenbrock_chain(int ncells, int ld, double* var, const double* fix,

@@ -11,6 +11,9 @@
 //                      sequence as the loop of util/sutil.c:2-23
 //   kpp_solve          unrolled forward/backward substitution
 //                      (src/gen.c:1960-2034)
+// and a second header, <prefix>_cmplx.cuh, with the complex LU the
+// Runge-Kutta methods factorise (KppDecompCmplxR / KppSolveCmplxR of
+// util/sutil.c:28-90, unrolled in the same operation order).
 //
 // Arithmetic is the reference's, operation for operation: expression trees
 // are built with the same constant folding (multiplying by a constant 1
@@ -867,6 +870,117 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     o << "  X[" << i << "] = " << print(sum) << ";\n";
   }
   o << "}\n\n";
+
+  // ---- KppDecompCmplxR / KppSolveCmplxR (util/sutil.c:28-90), unrolled.
+  // The reference runs these generic loops over LU_CROW / LU_ICOL / LU_DIAG
+  // with a dense work row; the elimination reads only row k's own pattern
+  // entries and the finished rows above it, so working in place on row k
+  // performs the same operations on the same values.
+  long ops_decomp_c = 0, ops_solve_c = 0;
+  std::ostringstream oc;  // written to <prefix>_cmplx.cuh
+  {
+    std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
+    for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
+    const bool chunked = m.lu_nonzero >= 2000;
+    const int kChunkOps = 1200;
+    std::vector<int> starts = {0};
+    if (chunked) {
+      int acc = 0;
+      for (int k = 0; k < nvar; k++) {
+        int row_ops = 0;
+        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+          int j = m.lu_icol[kk];
+          row_ops += 1 + 2 * (m.lu_crow[j + 1] - m.lu_diag[j] - 1);
+        }
+        if (acc > 0 && acc + row_ops > kChunkOps) {
+          starts.push_back(k);
+          acc = 0;
+        }
+        acc += row_ops;
+      }
+    }
+    starts.push_back(nvar);
+    const int nchunks = (int)starts.size() - 1;
+    const char* head =
+        "// In-place no-pivot sparse LU of the complex matrix (JR + i JI) of one cell;\n"
+        "// returns k+1 when the real or the imaginary part of row k's diagonal entry\n"
+        "// is zero on entry to its elimination, 0 on success.\n";
+    for (int c = 0; c < nchunks; c++) {
+      if (nchunks > 1)
+        oc << "// Rows " << starts[c] << ".." << starts[c + 1] - 1 << " of the complex LU.\n"
+          << "template <class TJ>\n"
+          << "__device__ __noinline__ int kpp_decomp_cmplx_rows" << c << "(TJ& JR, TJ& JI) {\n";
+      else
+        oc << head << "template <class TJ>\n"
+          << "__device__ KPP_MECH_INLINE int kpp_decomp_cmplx(TJ& JR, TJ& JI) {\n";
+      oc << "  double ar, ai, den;\n";
+      for (int k = starts[c]; k < starts[c + 1]; k++) {
+        const int dk = m.lu_diag[k];
+        oc << "  if (JR[" << dk << "] == 0.0) return " << (k + 1) << ";\n"
+          << "  if (JI[" << dk << "] == 0.0) return " << (k + 1) << ";\n";
+        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+          const int j = m.lu_icol[kk], dj = m.lu_diag[j];
+          ops_decomp_c += 3 + 8;
+          oc << "  den = JR[" << dj << "]*JR[" << dj << "] + JI[" << dj << "]*JI[" << dj << "];\n"
+            << "  ar = -(JR[" << kk << "]*JR[" << dj << "] + JI[" << kk << "]*JI[" << dj
+            << "])/den;\n"
+            << "  ai = -(JI[" << kk << "]*JR[" << dj << "] - JR[" << kk << "]*JI[" << dj
+            << "])/den;\n"
+            << "  JR[" << kk << "] = -ar;\n  JI[" << kk << "] = -ai;\n";
+          for (int jj = dj + 1; jj < m.lu_crow[j + 1]; jj++) {
+            const int t = pos[k][m.lu_icol[jj]];
+            ops_decomp_c += 8;
+            oc << "  JR[" << t << "] = JR[" << t << "] + ar*JR[" << jj << "] - ai*JI[" << jj
+              << "];\n"
+              << "  JI[" << t << "] = JI[" << t << "] + ar*JI[" << jj << "] + ai*JR[" << jj
+              << "];\n";
+          }
+        }
+      }
+      oc << "  (void)ar; (void)ai; (void)den;\n  return 0;\n}\n\n";
+    }
+    if (nchunks > 1) {
+      oc << head << "template <class TJ>\n"
+        << "__device__ KPP_MECH_INLINE int kpp_decomp_cmplx(TJ& JR, TJ& JI) {\n  int r;\n";
+      for (int c = 0; c < nchunks; c++)
+        oc << "  if ((r = kpp_decomp_cmplx_rows" << c << "(JR, JI)) != 0) return r;\n";
+      oc << "  return 0;\n}\n\n";
+    }
+
+    oc << "// Solve (LU) x = b in place for the complex LU of kpp_decomp_cmplx, b given\n"
+         "// in (XR, XI).\n"
+         "template <class TJ, class TX>\n"
+         "__device__ KPP_MECH_INLINE void kpp_solve_cmplx(const TJ& JR, const TJ& JI, TX& XR,"
+         " TX& XI) {\n"
+         "  double sumr, sumi, den;\n";
+    for (int i = 0; i < nvar; i++)
+      for (int j = m.lu_crow[i]; j < m.lu_diag[i]; j++) {
+        const int c = m.lu_icol[j];
+        ops_solve_c += 8;
+        oc << "  XR[" << i << "] = XR[" << i << "] - (JR[" << j << "]*XR[" << c << "] - JI[" << j
+          << "]*XI[" << c << "]);\n"
+          << "  XI[" << i << "] = XI[" << i << "] - (JR[" << j << "]*XI[" << c << "] + JI[" << j
+          << "]*XR[" << c << "]);\n";
+      }
+    for (int i = nvar - 1; i >= 0; i--) {
+      const int d = m.lu_diag[i];
+      oc << "  sumr = XR[" << i << "];\n  sumi = XI[" << i << "];\n";
+      for (int j = d + 1; j < m.lu_crow[i + 1]; j++) {
+        const int c = m.lu_icol[j];
+        ops_solve_c += 8;
+        oc << "  sumr = sumr - (JR[" << j << "]*XR[" << c << "] - JI[" << j << "]*XI[" << c
+          << "]);\n"
+          << "  sumi = sumi - (JR[" << j << "]*XI[" << c << "] + JI[" << j << "]*XR[" << c
+          << "]);\n";
+      }
+      ops_solve_c += 11;
+      oc << "  den = JR[" << d << "]*JR[" << d << "] + JI[" << d << "]*JI[" << d << "];\n"
+        << "  XR[" << i << "] = (sumr*JR[" << d << "] + sumi*JI[" << d << "])/den;\n"
+        << "  XI[" << i << "] = (sumi*JR[" << d << "] - sumr*JI[" << d << "])/den;\n";
+    }
+    oc << "  (void)sumr; (void)sumi; (void)den;\n}\n\n";
+  }
+
   o << "// FP64 add/sub/mul/div operations per call of each function (for the\n"
        "// FP64 roofline; rate constants and the integrator's vector operations\n"
        "// are counted separately).\n"
@@ -874,13 +988,23 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     << "#define KPP_OPS_JAC " << ops_jac << "\n"
     << "#define KPP_OPS_DECOMP " << ops_decomp << "\n"
     << "#define KPP_OPS_SOLVE " << ops_solve << "\n";
+  oc << "#define KPP_OPS_DECOMP_CMPLX " << ops_decomp_c << "\n"
+     << "#define KPP_OPS_SOLVE_CMPLX " << ops_solve_c << "\n";
 
   emit_warp_tables(o, m);
 
   std::ofstream f(out_prefix + ".cuh");
   if (!f) return false;
   f << o.str();
-  return (bool)f;
+  if (!f) return false;
+  // The complex LU lives in a header of its own, included after the main one
+  // only by the integrators that need it (the Runge-Kutta methods).
+  std::ofstream fc(out_prefix + "_cmplx.cuh");
+  if (!fc) return false;
+  fc << "// Generated by kppcu: complex sparse LU of the mechanism (util/sutil.c:28-90),\n"
+        "// unrolled.  Include after the mechanism header.\n#pragma once\n\n"
+     << oc.str();
+  return (bool)fc;
 }
 
 }  // namespace kppcu

@@ -97,6 +97,7 @@ class Mechanism:
         L.kpp_b200_sdirk.argtypes = ([ctypes.c_int, ctypes.c_int] + [_vp] * 9
                                      + [ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double)] + [_vp] * 4)
+        L.kpp_b200_runge_kutta.argtypes = L.kpp_b200_sdirk.argtypes
         L.kpp_b200_user_species.argtypes = [_vp, _vp]
         L.kpp_b200_shuffle_user2kpp.argtypes = [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                 _vp, _vp]
@@ -249,6 +250,35 @@ class Mechanism:
         rc = (ctypes.c_double * 20)(*[float(x) for x in rcntrl])
         s = stream if stream is not None else torch.cuda.current_stream(var.device)
         self._check(self.lib.kpp_b200_sdirk(
+            n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
+            _ptr(tend), _ptr(atol), _ptr(rtol), ic, rc, _ptr(out.istatus), _ptr(out.rstatus),
+            _ptr(out.ierr), _vp(s.cuda_stream)))
+        return out
+
+    def runge_kutta(self, var: torch.Tensor, fix: torch.Tensor, temp: torch.Tensor,
+                    tstart: torch.Tensor, tend: torch.Tensor, atol: torch.Tensor,
+                    rtol: torch.Tensor, icntrl: Sequence[int], rcntrl: Sequence[float],
+                    cfactor: Optional[torch.Tensor] = None, sun: Optional[torch.Tensor] = None,
+                    ncells: Optional[int] = None, out: Optional[RosenbrockResult] = None,
+                    stream: Optional[torch.cuda.Stream] = None) -> RosenbrockResult:
+        """The reference's C RungeKutta integrator for every cell
+        (kpp_b200_runge_kutta): ICNTRL / RCNTRL in the C layout; istatus =
+        ISTATUS[0..7], rstatus [3, ld] = RSTATUS[0..2] (Texit, Hacc, Hnew)."""
+        f64, i32 = torch.float64, torch.int32
+        self._dev(var, f64, "var")
+        ld = var.shape[1]
+        n = ld if ncells is None else ncells
+        for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                      (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun")):
+            self._dev(t, f64, nm)
+        if out is None:
+            out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
+                                   istatus=torch.empty(8, ld, dtype=i32, device=var.device),
+                                   rstatus=torch.empty(3, ld, dtype=f64, device=var.device))
+        ic = (ctypes.c_int * 20)(*[int(x) for x in icntrl])
+        rc = (ctypes.c_double * 20)(*[float(x) for x in rcntrl])
+        s = stream if stream is not None else torch.cuda.current_stream(var.device)
+        self._check(self.lib.kpp_b200_runge_kutta(
             n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
             _ptr(tend), _ptr(atol), _ptr(rtol), ic, rc, _ptr(out.istatus), _ptr(out.rstatus),
             _ptr(out.ierr), _vp(s.cuda_stream)))

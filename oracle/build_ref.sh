@@ -12,8 +12,10 @@
 #   oracle/_ref/<mech>/libkppref_<mech>.so        -O (reference flags, util/Makefile_c:3)
 #   oracle/_ref/<mech>/libkppref_<mech>_O3.so     -O3 -march=x86-64-v3 (FMA contraction:
 #                                                 the same code with another valid rounding)
-#   oracle/_ref/<mech>_sdirk/libkppsd_<mech>[_O3].so  the model with the reference SDIRK
-#                                                 integrator (int/sdirk.c)
+#   oracle/_ref/<mech>_sdirk/libkppsd_<mech>[_O3|_pw].so  the model with the reference
+#                                                 SDIRK integrator (int/sdirk.c)
+#   oracle/_ref/<mech>_rk/libkpprk_<mech>[_O3|_pw].so  ... with the reference Runge-Kutta
+#                                                 integrator (int/runge_kutta.c)
 #
 # The generator is compiled from the unchanged sources in $KPP_REF/src; only
 # the flex/bison front end is replaced by oracle/refkpp/frontend.c because
@@ -45,6 +47,57 @@ done
 "$CC" "$OUT"/obj/*.o -lm -o "$OUT/kpp"
 
 # ---- 2. per-mechanism reference model ---------------------------------------
+# build_integrator_model MECH INTEGRATOR DRIVER TAG PREFIX: the model with
+# another reference integrator and its batch driver (refkpp/DRIVER.c) in
+# oracle/_ref/MECH_TAG/: libPREFIX_MECH.so (reference flags), _O3 (FMA
+# contraction) and _pw (the integrator's pow() through the driver's
+# kppref_pow, refkpp/pow_knob.h, and Update_SUN's cos() through kppref_cos,
+# refkpp/cos_knob.h; each can move its result one ulp: other valid
+# roundings of pow and cos).
+build_integrator_model() {
+  local mech="$1" integ="$2" driver="$3" tag="$4" prefix="$5"
+  local ds="$OUT/${mech}_${tag}"
+  rm -rf "$ds"
+  mkdir -p "$ds"
+  cat > "$ds/$mech.kpp" <<EOF
+#MODEL      $mech
+#LANGUAGE   C
+#DOUBLE     ON
+#INTEGRATOR $integ
+#DRIVER     $HERE/refkpp/$driver
+#JACOBIAN   SPARSE_LU_ROW
+#HESSIAN    OFF
+#STOICMAT   OFF
+#MEX        OFF
+#INLINE C_GLOBAL
+  extern double kppref_sun_override;
+  extern int kppref_sun_ulps;
+#ENDINLINE
+#INLINE C_RCONST
+  if (kppref_sun_override >= 0.0) SUN = kppref_sun_override;
+  if (kppref_sun_ulps > 0) SUN = nextafter(SUN, 2.0);
+  if (kppref_sun_ulps < 0) SUN = nextafter(SUN, -1.0);
+#ENDINLINE
+EOF
+  (cd "$ds" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
+    echo "build_ref: kpp ($integ) failed for $mech" >&2; tail -20 "$ds/kpp.log" >&2; exit 1; }
+  local srcs=() others=() f
+  for f in "$ds/${mech}"_*.c; do
+    case "$f" in *_mex_*) ;; *) srcs+=("$f") ;; esac
+  done
+  "$CC" -O -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm -o "$ds/lib${prefix}_${mech}.so"
+  "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm \
+    -o "$ds/lib${prefix}_${mech}_O3.so"
+  for f in "${srcs[@]}"; do
+    case "$f" in *_Integrator.c|*_Rates.c) ;; *) others+=("$f") ;; esac
+  done
+  "$CC" -O -w -fPIC -c -include "$HERE/refkpp/pow_knob.h" -I"$ds" "$ds/${mech}_Integrator.c" -o "$ds/integrator_pw.o"
+  "$CC" -O -w -fPIC -c -include "$HERE/refkpp/cos_knob.h" -I"$ds" "$ds/${mech}_Rates.c" -o "$ds/rates_pw.o"
+  "$CC" -O -w -fPIC -shared -I"$ds" "${others[@]}" "$ds/integrator_pw.o" "$ds/rates_pw.o" -lm \
+    -o "$ds/lib${prefix}_${mech}_pw.so"
+  echo "build_ref: $mech ($integ) -> $ds/lib${prefix}_${mech}.so"
+}
+
 for mech in "${MECHS[@]}"; do
   d="$OUT/$mech"
   rm -rf "$d"
@@ -109,53 +162,11 @@ EOF
   fi
   echo "build_ref: $mech -> $d/libkppref_${mech}.so"
 
-  # the same model with the reference SDIRK integrator (int/sdirk.c) and its
-  # batch driver, for the SDIRK entry's parity tests
+  # the same model with the reference SDIRK (int/sdirk.c) and Runge-Kutta
+  # (int/runge_kutta.c) integrators and their batch drivers, for those
+  # entries' parity tests
   if [ "$mech" != "mcm_isoprene" ]; then
-    ds="$OUT/${mech}_sdirk"
-    rm -rf "$ds"
-    mkdir -p "$ds"
-    cat > "$ds/$mech.kpp" <<EOF
-#MODEL      $mech
-#LANGUAGE   C
-#DOUBLE     ON
-#INTEGRATOR sdirk
-#DRIVER     $HERE/refkpp/batch_driver_sdirk
-#JACOBIAN   SPARSE_LU_ROW
-#HESSIAN    OFF
-#STOICMAT   OFF
-#MEX        OFF
-#INLINE C_GLOBAL
-  extern double kppref_sun_override;
-  extern int kppref_sun_ulps;
-#ENDINLINE
-#INLINE C_RCONST
-  if (kppref_sun_override >= 0.0) SUN = kppref_sun_override;
-  if (kppref_sun_ulps > 0) SUN = nextafter(SUN, 2.0);
-  if (kppref_sun_ulps < 0) SUN = nextafter(SUN, -1.0);
-#ENDINLINE
-EOF
-    (cd "$ds" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
-      echo "build_ref: kpp (sdirk) failed for $mech" >&2; tail -20 "$ds/kpp.log" >&2; exit 1; }
-    srcs=()
-    for f in "$ds/${mech}"_*.c; do
-      case "$f" in *_mex_*) ;; *) srcs+=("$f") ;; esac
-    done
-    "$CC" -O -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm -o "$ds/libkppsd_${mech}.so"
-    "$CC" -O3 -march=x86-64-v3 -ffp-contract=fast -w -fPIC -shared -I"$ds" "${srcs[@]}" -lm \
-      -o "$ds/libkppsd_${mech}_O3.so"
-    # the integrator's pow() calls (step-size factor, Newton tests, SQRT of
-    # the error norm) through the driver's kppsd_pow (refkpp/pow_knob.h), and
-    # Update_SUN's cos() through kppsd_cos (refkpp/cos_knob.h); each can move
-    # its result one ulp: other valid roundings of pow and cos
-    others=()
-    for f in "${srcs[@]}"; do
-      case "$f" in *_Integrator.c|*_Rates.c) ;; *) others+=("$f") ;; esac
-    done
-    "$CC" -O -w -fPIC -c -include "$HERE/refkpp/pow_knob.h" -I"$ds" "$ds/${mech}_Integrator.c" -o "$ds/integrator_pw.o"
-    "$CC" -O -w -fPIC -c -include "$HERE/refkpp/cos_knob.h" -I"$ds" "$ds/${mech}_Rates.c" -o "$ds/rates_pw.o"
-    "$CC" -O -w -fPIC -shared -I"$ds" "${others[@]}" "$ds/integrator_pw.o" "$ds/rates_pw.o" -lm \
-      -o "$ds/libkppsd_${mech}_pw.so"
-    echo "build_ref: $mech (sdirk) -> $ds/libkppsd_${mech}.so"
+    build_integrator_model "$mech" sdirk batch_driver_sdirk sdirk kppsd
+    build_integrator_model "$mech" runge_kutta batch_driver_rk rk kpprk
   fi
 done

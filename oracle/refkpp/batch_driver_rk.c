@@ -1,0 +1,102 @@
+/*~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+  Batch driver for the reference's own KPP-generated C model with the
+  reference fully implicit Runge-Kutta integrator (#INTEGRATOR runge_kutta,
+  int/runge_kutta.c).
+
+  ORACLE INFRASTRUCTURE ONLY -- built by oracle/build_ref.sh into
+  oracle/_ref/<mech>_rk/libkpprk_<mech>[_O3|_pw].so and loaded only by tests
+  and the CPU legs of bench.py.
+
+  Given to the generator with #DRIVER (src/gen.c:2564-2581) in place of the
+  stock drv/general.c: it loops over a batch of independent cells, sets the
+  generator's globals for each cell (C = VAR|FIX, TEMP, CFACTOR, TIME) and
+  calls RungeKutta(NVAR, Tstart, Tend, VAR, RTOL, ATOL, RCNTRL, ICNTRL,
+  RSTATUS, ISTATUS, &IERR) as INTEGRATE does (int/runge_kutta.c:114-198),
+  with the caller's ICNTRL / RCNTRL (RungeKutta clears ISTATUS / RSTATUS
+  itself).  Per-cell sunlight as in batch_driver.c.
+
+  Array layout: structure of arrays, cell index fastest, leading dimension ld.
+  ISTATUS[0..7] and RSTATUS[0..2] come back as rows 0..7 of istatus and 0..2
+  of rstatus.  The reference loops without end when a cell's step size
+  becomes 0 or NaN: callers give it only inputs it finishes.
+~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~*/
+
+double kppref_sun_override = -1.0;
+int kppref_sun_ulps = 0;
+
+/* Test knob: every evaluation moves SUN by one ulp up (1) or down (-1). */
+void kpprk_set_sun_ulps(int u) { kppref_sun_ulps = u; }
+
+/* The integrator's pow() in the libkpprk_<mech>_pw.so build (pow_knob.h
+   force-included): libm's pow, moved one ulp up (1) or down (-1) on request;
+   a constant exponent 2 gives x*x as in the plain build. */
+static int kppref_pow_ulps = 0;
+void kppref_set_pow_ulps(int u) { kppref_pow_ulps = u; }
+double kppref_pow(double x, double y, int square)
+{
+  double r = square ? x * x : pow(x, y);
+  if (kppref_pow_ulps > 0) r = nextafter(r, HUGE_VAL);
+  if (kppref_pow_ulps < 0) r = nextafter(r, -HUGE_VAL);
+  return r;
+}
+
+/* Update_SUN's cos() in the same build (cos_knob.h force-included into the
+   Rates file): libm's cos, moved one ulp up (1) or down (-1) on request. */
+static int kppref_cos_ulps = 0;
+void kppref_set_cos_ulps(int u) { kppref_cos_ulps = u; }
+double kppref_cos(double x)
+{
+  double r = cos(x);
+  if (kppref_cos_ulps > 0) r = nextafter(r, HUGE_VAL);
+  if (kppref_cos_ulps < 0) r = nextafter(r, -HUGE_VAL);
+  return r;
+}
+
+void RungeKutta(int N, double T, double Tend, double Y[], double RelTol[], double AbsTol[],
+                double RCNTRL[], int ICNTRL[], double RSTATUS[], int ISTATUS[], int *IERR);
+
+int kpprk_dims(int *d)
+{
+  d[0] = NVAR; d[1] = NFIX; d[2] = NSPEC; d[3] = NREACT; d[4] = LU_NONZERO;
+  return 0;
+}
+
+/* The reference's complex sparse LU and solve (util/sutil.c:28-90) of the
+   generated model, for the tests of the generated device version. */
+int kpprk_decomp_cmplx(double *jr, double *ji) { return KppDecompCmplxR(jr, ji); }
+void kpprk_solve_cmplx(double *jr, double *ji, double *xr, double *xi)
+{
+  KppSolveCmplxR(jr, ji, xr, xi);
+}
+
+int kpprk_integrate(int ncells, int ld, double *var, const double *fix,
+                    const double *temp, const double *cfactor, const double *sun,
+                    const double *tstart, const double *tend, const double *atol,
+                    const double *rtol, const int *icntrl, const double *rcntrl,
+                    int *istatus, double *rstatus, int *ierr)
+{
+  double at[NVAR], rt[NVAR], rc[20], rs[20];
+  int ic[20], is[20];
+  int cell, i, e;
+  const int nt = icntrl[1] == 0 ? NVAR : 1;  /* vector or scalar tolerances */
+  for (i = 0; i < NVAR; i++) { at[i] = atol[i < nt ? i : 0]; rt[i] = rtol[i < nt ? i : 0]; }
+  for (cell = 0; cell < ncells; cell++) {
+    for (i = 0; i < 20; i++) { ic[i] = icntrl[i]; rc[i] = rcntrl[i]; is[i] = 0; rs[i] = 0.0; }
+    for (i = 0; i < NVAR; i++) VAR[i] = var[(long)i * ld + cell];
+    /* NSPEC - NVAR real fixed species (KPP pads NFIX to 1 when there are none) */
+    for (i = 0; i < NSPEC - NVAR; i++) FIX[i] = fix[(long)i * ld + cell];
+    TEMP = temp[cell];
+    if (cfactor) CFACTOR = cfactor[cell];
+    kppref_sun_override = sun ? sun[cell] : -1.0;
+    TIME = tstart[cell];
+
+    e = 0;
+    RungeKutta(NVAR, tstart[cell], tend[cell], VAR, rt, at, rc, ic, rs, is, &e);
+    ierr[cell] = e;
+
+    for (i = 0; i < NVAR; i++) var[(long)i * ld + cell] = VAR[i];
+    for (i = 0; i < 8; i++) istatus[(long)i * ld + cell] = is[i];
+    for (i = 0; i < 3; i++) rstatus[(long)i * ld + cell] = rs[i];
+  }
+  return 0;
+}

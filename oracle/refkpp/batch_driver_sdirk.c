@@ -26,15 +26,15 @@ void kppsd_set_sun_ulps(int u) { kppref_sun_ulps = u; }
 
 /* The integrator's pow() in the libkppsd_<mech>_pw.so build (pow_knob.h
    force-included): libm's pow, moved one ulp up (1) or down (-1) on request.
-   pow(x, 2) is x*x, as the compiler folds it in the plain build, so that the
-   knob at 0 reproduces the plain build bit for bit. */
-static int kppsd_pow_ulps = 0;
-void kppsd_set_pow_ulps(int u) { kppsd_pow_ulps = u; }
-double kppsd_pow(double x, double y)
+   A constant exponent 2 gives x*x, as the compiler folds pow(x, 2) in the
+   plain build, so that the knob at 0 reproduces the plain build bit for bit. */
+static int kppref_pow_ulps = 0;
+void kppref_set_pow_ulps(int u) { kppref_pow_ulps = u; }
+double kppref_pow(double x, double y, int square)
 {
-  double r = (y == 2.0) ? x * x : pow(x, y);
-  if (kppsd_pow_ulps > 0) r = nextafter(r, HUGE_VAL);
-  if (kppsd_pow_ulps < 0) r = nextafter(r, -HUGE_VAL);
+  double r = square ? x * x : pow(x, y);
+  if (kppref_pow_ulps > 0) r = nextafter(r, HUGE_VAL);
+  if (kppref_pow_ulps < 0) r = nextafter(r, -HUGE_VAL);
   return r;
 }
 

@@ -149,28 +149,46 @@ def alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, ipar, rpar, 
     return np.stack(out)
 
 
+_INTEGRATORS = {"sdirk": ("sdirk", "kppsd"), "rk": ("rk", "kpprk")}
+
+
+def integrator_lib_path(kind: str, mech: str, opt: str = "") -> Path:
+    tag, prefix = _INTEGRATORS[kind]
+    return REF_DIR / f"{mech}_{tag}" / f"lib{prefix}_{mech}{opt}.so"
+
+
 def sdirk_lib_path(mech: str, opt: str = "") -> Path:
-    return REF_DIR / f"{mech}_sdirk" / f"libkppsd_{mech}{opt}.so"
+    return integrator_lib_path("sdirk", mech, opt)
 
 
-class SdirkOracle:
-    """The reference's own C SDIRK (int/sdirk.c) on the mechanism's generated
-    model, per cell through oracle/refkpp/batch_driver_sdirk.c."""
+def rk_lib_path(mech: str, opt: str = "") -> Path:
+    return integrator_lib_path("rk", mech, opt)
+
+
+class IntegratorOracle:
+    """The reference's own C SDIRK (int/sdirk.c) or Runge-Kutta
+    (int/runge_kutta.c) integrator on the mechanism's generated model, per
+    cell through oracle/refkpp/batch_driver_sdirk.c / batch_driver_rk.c."""
+
+    kind = "sdirk"
 
     def __init__(self, mech: str, opt: str = ""):
-        self.lib = ctypes.CDLL(str(sdirk_lib_path(mech, opt)))
-        self.lib.kppsd_integrate.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 14
+        self.prefix = _INTEGRATORS[self.kind][1]
+        self.lib = ctypes.CDLL(str(integrator_lib_path(self.kind, mech, opt)))
+        self._integrate = getattr(self.lib, f"{self.prefix}_integrate")
+        self._integrate.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 14
         d = (ctypes.c_int * 5)()
-        self.lib.kppsd_dims(d)
-        self.nvar = d[0]
-        self.lib.kppsd_set_sun_ulps.argtypes = [ctypes.c_int]
+        getattr(self.lib, f"{self.prefix}_dims")(d)
+        self.nvar, self.lu_nonzero = d[0], d[4]
+        self._sun = getattr(self.lib, f"{self.prefix}_set_sun_ulps")
+        self._sun.argtypes = [ctypes.c_int]
 
     def set_sun_ulps(self, u: int):
-        self.lib.kppsd_set_sun_ulps(u)
+        self._sun(u)
 
     def set_pow_ulps(self, u: int):
         """Moves the integrator's pow() results one ulp (the `_pw` build only)."""
-        self.lib.kppsd_set_pow_ulps(ctypes.c_int(u))
+        self.lib.kppref_set_pow_ulps(ctypes.c_int(u))
 
     def set_cos_ulps(self, u: int):
         """Moves Update_SUN's cos() results one ulp (the `_pw` build only)."""
@@ -178,8 +196,9 @@ class SdirkOracle:
 
     def integrate(self, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl, cfactor=None,
                   sun=None):
-        """Returns (var_out, istatus [8][n] = ISTATUS[1..8], rstatus [3][n] =
-        RSTATUS[1..3], ierr)."""
+        """Returns (var_out, istatus [8][n], rstatus [3][n], ierr): SDIRK's
+        ISTATUS[1..8] / RSTATUS[1..3], Runge-Kutta's ISTATUS[0..7] /
+        RSTATUS[0..2]."""
         var = np.ascontiguousarray(var, dtype=np.float64).copy()
         n = var.shape[1]
         f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
@@ -191,38 +210,61 @@ class SdirkOracle:
         ist = np.zeros((8, n), np.int32)
         rst = np.zeros((3, n))
         ierr = np.zeros(n, np.int32)
-        self.lib.kppsd_integrate(n, n, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun),
-                                 _p(tstart), _p(tend), _p(atol), _p(rtol), _p(ic), _p(rc),
-                                 _p(ist), _p(rst), _p(ierr))
+        self._integrate(n, n, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun), _p(tstart),
+                        _p(tend), _p(atol), _p(rtol), _p(ic), _p(rc), _p(ist), _p(rst),
+                        _p(ierr))
         return var, ist, rst, ierr
 
 
-def sdirk_alternates(mech: str, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
-                     cfactor=None, sun=None):
-    """VAR after the same SDIRK integration by the reference under other
-    valid last-ulp roundings: compiled with FMA contraction; SUN one ulp up
-    and down at every evaluation; the integrator's pow() one ulp up and down
-    (the step-size factor and the Newton convergence tests decide on it);
-    Update_SUN's cos() one ulp up and down (SUN = (1 + cos)/2 cancels near
-    sunrise and sunset, where a one-ulp cosine moves SUN far more than one
-    ulp of SUN does)."""
-    out = [SdirkOracle(mech, "_O3").integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl,
-                                              rcntrl, cfactor=cfactor, sun=sun)[0]]
-    o = SdirkOracle(mech)
+class SdirkOracle(IntegratorOracle):
+    kind = "sdirk"
+
+
+class RkOracle(IntegratorOracle):
+    kind = "rk"
+
+    def decomp_cmplx(self, jr, ji):
+        """The reference's KppDecompCmplxR (util/sutil.c:28-59) in place."""
+        return int(self.lib.kpprk_decomp_cmplx(_p(jr), _p(ji)))
+
+    def solve_cmplx(self, jr, ji, xr, xi):
+        """The reference's KppSolveCmplxR (util/sutil.c:64-87) in place."""
+        self.lib.kpprk_solve_cmplx(_p(jr), _p(ji), _p(xr), _p(xi))
+
+
+def integrator_alternates(kind: str, mech: str, var, fix, temp, tstart, tend, atol, rtol,
+                          icntrl, rcntrl, cfactor=None, sun=None):
+    """VAR after the same SDIRK or Runge-Kutta integration by the reference
+    under other valid last-ulp roundings: compiled with FMA contraction; SUN
+    one ulp up and down at every evaluation; the integrator's pow() one ulp
+    up and down (the step-size factor and the Newton convergence tests decide
+    on it); Update_SUN's cos() one ulp up and down (SUN = (1 + cos)/2 cancels
+    near sunrise and sunset, where a one-ulp cosine moves SUN far more than
+    one ulp of SUN does)."""
+    cls = SdirkOracle if kind == "sdirk" else RkOracle
+    args = (var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl)
+    out = [cls(mech, "_O3").integrate(*args, cfactor=cfactor, sun=sun)[0]]
+    o = cls(mech)
     for u in (1, -1):
         o.set_sun_ulps(u)
         try:
-            out.append(o.integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
-                                   cfactor=cfactor, sun=sun)[0])
+            out.append(o.integrate(*args, cfactor=cfactor, sun=sun)[0])
         finally:
             o.set_sun_ulps(0)
-    pw = SdirkOracle(mech, "_pw")
+    pw = cls(mech, "_pw")
     for knob in (pw.set_pow_ulps, pw.set_cos_ulps):
         for u in (1, -1):
             knob(u)
             try:
-                out.append(pw.integrate(var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
-                                        cfactor=cfactor, sun=sun)[0])
+                out.append(pw.integrate(*args, cfactor=cfactor, sun=sun)[0])
             finally:
                 knob(0)
     return np.stack(out)
+
+
+def sdirk_alternates(mech: str, *args, **kw):
+    return integrator_alternates("sdirk", mech, *args, **kw)
+
+
+def rk_alternates(mech: str, *args, **kw):
+    return integrator_alternates("rk", mech, *args, **kw)

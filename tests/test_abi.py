@@ -93,6 +93,15 @@ def test_entry_points_reject_bad_arguments_without_gpu():
     assert rc == 1 and b"null" in lib.kpp_b200_last_error()
     assert lib.kpp_b200_sdirk(0, 0, None, None, None, None, None, None, None, None, None, ip, rp,
                               None, None, None, None) == 0
+    # and the Runge-Kutta entry
+    rc = lib.kpp_b200_runge_kutta(4, 2, None, None, None, None, None, None, None, None, None, ip,
+                                  rp, None, None, None, None)
+    assert rc == 1 and b"ncells" in lib.kpp_b200_last_error()
+    rc = lib.kpp_b200_runge_kutta(4, 4, None, None, None, None, None, None, None, None, None, ip,
+                                  rp, None, None, None, None)
+    assert rc == 1 and b"null" in lib.kpp_b200_last_error()
+    assert lib.kpp_b200_runge_kutta(0, 0, None, None, None, None, None, None, None, None, None,
+                                    ip, rp, None, None, None, None) == 0
 
 
 def test_controls_layouts():

@@ -1,0 +1,212 @@
+"""GPU parity of the Runge-Kutta integrator (int/runge_kutta.c of the
+reference) against the reference's own C RungeKutta on the same generated
+model.
+
+The reference is the mechanism generated with `#INTEGRATOR runge_kutta` and
+driven cell by cell (oracle/refkpp/batch_driver_rk.c).  The bar is the one
+of the other integrators: identical IERR per cell, concentrations within
+1e-9 relative (or within 30x the reference's own spread under valid last-ulp
+roundings: FMA contraction, SUN one ulp up / down, the integrator's pow()
+and Update_SUN's cos() one ulp up / down), and the same integrator
+statistics for almost every cell.
+"""
+import numpy as np
+import pytest
+import torch
+
+from kpp_b200 import workloads
+from parity import assert_var_parity, max_rel_err
+from test_rk_host import rk_controls
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+
+def oracle(mech):
+    from oracle_lib import RkOracle, rk_lib_path
+    for opt in ("", "_O3", "_pw"):
+        if not rk_lib_path(mech, opt).exists():
+            pytest.skip("Runge-Kutta oracle libraries not present")
+    return RkOracle(mech)
+
+
+def run_both(mech, ncells, seed, ic, rc, atol=None, rtol=None, step=0, window=None):
+    from kpp_b200 import load
+    from oracle_lib import rk_alternates
+    o = oracle(mech)
+    m = load(mech)
+    wl = workloads.for_mechanism(m, mech, ncells, seed=seed)
+    atol = wl.atol if atol is None else atol
+    rtol = wl.rtol if rtol is None else rtol
+    fix_ref = wl.fix if wl.fix.shape[0] else np.zeros((1, ncells))  # the C model pads NFIX
+    t0, t1 = wl.step_bounds(step)
+    if window is not None:
+        t1 = t0 + window
+    ref = o.integrate(wl.var, fix_ref, wl.temp, t0, t1, atol, rtol, ic, rc, cfactor=wl.cfactor,
+                      sun=wl.sun)
+    alt = rk_alternates(mech, wl.var, fix_ref, wl.temp, t0, t1, atol, rtol, ic, rc,
+                        cfactor=wl.cfactor, sun=wl.sun)
+    var = dev(wl.var)
+    r = m.runge_kutta(var, dev(wl.fix), dev(wl.temp), dev(t0), dev(t1), dev(atol), dev(rtol),
+                      ic, rc, cfactor=None if wl.cfactor is None else dev(wl.cfactor),
+                      sun=None if wl.sun is None else dev(wl.sun))
+    torch.cuda.synchronize()
+    got = (var.cpu().numpy(), r.istatus.cpu().numpy(), r.rstatus.cpu().numpy(),
+           r.ierr.cpu().numpy())
+    return got, ref, alt
+
+
+def check(got, ref, alt, what, stats_frac=0.95):
+    var, ist, rst, ierr = got
+    var_ref, ist_ref, rst_ref, ierr_ref = ref
+    np.testing.assert_array_equal(ierr, ierr_ref, err_msg=what)
+    assert_var_parity(var, var_ref, alt, what)
+    assert np.all(ist == ist_ref, axis=0).mean() >= stats_frac, what
+    ok = ierr_ref == 1
+    # Texit: the final time of every successful cell
+    assert max_rel_err(rst[0][ok], rst_ref[0][ok], floor=0) <= 1e-12, what
+
+
+@pytest.mark.parametrize("sdirk_error", [1, 0])
+@pytest.mark.parametrize("method", [0, 2, 3, 4])
+def test_every_rk_method_matches_reference(method, sdirk_error):
+    ic, rc = rk_controls(method=method, sdirk_error=sdirk_error)
+    got, ref, alt = run_both("small_strato", 512, 11, ic, rc)
+    assert (ref[3] == 1).all()
+    check(got, ref, alt, f"method {method} sdirk_error {sdirk_error}")
+
+
+@pytest.mark.parametrize("sdirk_error,window", [(1, 1e-6), (0, 1e-4)])
+def test_lobatto3a_short_windows_match_reference(sdirk_error, window):
+    ic, rc = rk_controls(method=5, sdirk_error=sdirk_error)
+    got, ref, alt = run_both("small_strato", 128, 11, ic, rc, window=window)
+    check(got, ref, alt, f"lobatto3a {sdirk_error}")
+
+
+@pytest.mark.parametrize("step", [0, 3, 6])
+def test_rk_diurnal_steps_match_reference(step):
+    ic, rc = rk_controls(method=0)
+    got, ref, alt = run_both("small_strato", 2048, 5, ic, rc, step=step)
+    check(got, ref, alt, f"step {step}")
+
+
+@pytest.mark.parametrize("method", [0, 3, 4])
+def test_rk_saprc99_matches_reference(method):
+    ic, rc = rk_controls(method=method)
+    got, ref, alt = run_both("saprc99", 256, 7, ic, rc)
+    check(got, ref, alt, f"saprc99 method {method}")
+
+
+def _controls_cases():
+    return [
+        ("bad_method", dict(method=9), {}),
+        ("classic_controller", dict(classic_controller=1), {}),
+        ("newton_maxit_1", dict(newton_maxit=1), {}),
+        ("newton_start_zero", dict(start_newton=1), {}),
+        ("hstart", dict(hstart=10.0), {}),
+        ("hmin", dict(hmin=1.0), {}),
+        ("hmax", dict(hmax=50.0), {}),
+        ("max_steps_3", dict(max_steps=3), {}),
+        ("neg_max_steps", dict(max_steps=-1), {}),
+        ("neg_newton_maxit", dict(newton_maxit=-2), {}),
+        ("facmax_below_1", dict(facmax=0.5), {}),
+        ("theta_min_2", dict(theta_min=2.0), {}),
+        ("newton_tol_tiny", dict(newton_tol=1e-17), {}),
+        ("qmin_2", dict(qmin=2.0), {}),
+        ("qmin_qmax", dict(qmin=0.5, qmax=2.0), {}),
+        ("tiny_rtol", dict(), {"rtol": 1e-17}),
+        ("zero_atol", dict(), {"atol": 0.0}),
+        ("vector_tol", dict(scalar_tol=False), {"vector": True}),
+    ]
+
+
+@pytest.mark.parametrize("name,ctl,tol", _controls_cases(), ids=[c[0] for c in _controls_cases()])
+def test_rk_error_codes_and_controls_match_reference(name, ctl, tol):
+    from kpp_b200 import load
+    nv = load("small_strato").nvar
+    ic, rc = rk_controls(**ctl)
+    if tol.get("vector"):
+        atol = np.linspace(0.5, 2.0, nv)
+        rtol = np.linspace(1e-4, 1e-3, nv)
+    else:
+        atol = np.array([tol.get("atol", 1.0)])
+        rtol = np.array([tol.get("rtol", 1e-3)])
+    got, ref, alt = run_both("small_strato", 64, 3, ic, rc, atol=atol, rtol=rtol)
+    check(got, ref, alt, name)
+
+
+@pytest.mark.parametrize("mech,ncells", [("small_strato", 8192), ("saprc99", 2048)])
+def test_rk_cell_results_independent_of_batch(mech, ncells):
+    """A cell's result depends on nothing but its own inputs: not on the other
+    cells of the batch, their order, or what an earlier launch left in the
+    work arrays (one Newton iteration allowed: many rejected steps, and the
+    interpolated Newton start reads the previous step's polynomial)."""
+    from kpp_b200 import load
+    m = load(mech)
+    wl = workloads.for_mechanism(m, mech, ncells, seed=21)
+    ic, rc = rk_controls(method=0, newton_maxit=2)
+    t0, t1 = wl.step_bounds(0)
+    cf = None if wl.cfactor is None else dev(wl.cfactor)
+    sun = None if wl.sun is None else dev(wl.sun)
+
+    def run(idx):
+        sel = lambda a: None if a is None else a[..., idx]
+        var = dev(wl.var[:, idx])
+        r = m.runge_kutta(var, dev(wl.fix[:, idx]), dev(wl.temp[idx]), dev(t0[idx]),
+                          dev(t1[idx]), dev(wl.atol), dev(wl.rtol), ic, rc, cfactor=sel(cf),
+                          sun=sel(sun))
+        torch.cuda.synchronize()
+        return [x.cpu().numpy() for x in (var, r.istatus, r.rstatus, r.ierr)]
+
+    full = run(np.arange(ncells))
+    again = run(np.arange(ncells))
+    sub = np.random.default_rng(5).permutation(ncells)[: ncells // 3]
+    part = run(sub)
+    for a, b, c in zip(full, again, part):
+        np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(a[..., sub], c)
+    assert full[1][4].sum() > 0  # rejected steps: the path was taken
+
+
+def test_rk_empty_and_ragged_batches():
+    from kpp_b200 import load
+    m = load("small_strato")
+    ic, rc = rk_controls(method=0)
+    z = torch.zeros(0, dtype=torch.float64, device="cuda")
+    r = m.runge_kutta(torch.zeros(m.nvar, 0, dtype=torch.float64, device="cuda"),
+                      torch.zeros(m.nfix, 0, dtype=torch.float64, device="cuda"), z, z, z,
+                      dev(np.array([1.0])), dev(np.array([1e-3])), ic, rc)
+    assert r.ierr.numel() == 0
+    got, ref, alt = run_both("small_strato", 37, 13, ic, rc)
+    check(got, ref, alt, "ragged 37")
+    wl = workloads.for_mechanism(m, "small_strato", 37, seed=13)
+    ld = 64
+    var = torch.full((m.nvar, ld), -7.0, dtype=torch.float64, device="cuda")
+    var[:, :37] = dev(wl.var)
+    pad = lambda a: np.concatenate([a, np.ones(a.shape[:-1] + (ld - 37,))], axis=-1)
+    t0, t1 = wl.step_bounds(0)
+    r = m.runge_kutta(var, dev(pad(wl.fix)), dev(pad(wl.temp)), dev(pad(t0)), dev(pad(t1)),
+                      dev(wl.atol), dev(wl.rtol), ic, rc, ncells=37)
+    torch.cuda.synchronize()
+    assert torch.all(var[:, 37:] == -7.0)
+    np.testing.assert_array_equal(var[:, :37].cpu().numpy(), got[0])
+    assert torch.all(r.ierr[:37] == 1)
+
+
+def test_rk_not_built_for_large_mechanisms_reports_error():
+    """Mechanisms with LU_NONZERO >= 2000 (MCM) have no Runge-Kutta kernel:
+    the entry returns KPP_B200_EINVAL with a message, without a launch."""
+    from kpp_b200 import build, load
+    if not build.library_path("mcm_isoprene").exists():
+        pytest.skip("mcm_isoprene is built on request")
+    m = load("mcm_isoprene")
+    assert m.lu_nonzero >= 2000
+    ic, rc = rk_controls(method=0)
+    n = 32
+    d = lambda *s: torch.ones(*s, dtype=torch.float64, device="cuda")
+    with pytest.raises(RuntimeError, match="LU_NONZERO"):
+        m.runge_kutta(d(m.nvar, n), d(max(m.nfix, 1), n), d(n), d(n) * 0, d(n), d(1), d(1) * 1e-3,
+                      ic, rc)
