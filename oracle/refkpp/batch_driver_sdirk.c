@@ -30,11 +30,28 @@ void kppsd_set_sun_ulps(int u) { kppref_sun_ulps = u; }
    plain build, so that the knob at 0 reproduces the plain build bit for bit. */
 static int kppref_pow_ulps = 0;
 void kppref_set_pow_ulps(int u) { kppref_pow_ulps = u; }
+/* Knob 1 / -1: every result one ulp up / down.  Knob 2 / 3: one ulp up,
+   down or not, a direction hashed from the arguments (two different
+   hashes), as a pow whose last-ulp error varies from call to call does:
+   where the integrator's discrete decisions (accept, reuse the LU, Newton
+   converged) sit on a pow result, such errors change the step sequence. */
 double kppref_pow(double x, double y, int square)
 {
   double r = square ? x * x : pow(x, y);
-  if (kppref_pow_ulps > 0) r = nextafter(r, HUGE_VAL);
-  if (kppref_pow_ulps < 0) r = nextafter(r, -HUGE_VAL);
+  if (kppref_pow_ulps == 1) r = nextafter(r, HUGE_VAL);
+  if (kppref_pow_ulps == -1) r = nextafter(r, -HUGE_VAL);
+  if (kppref_pow_ulps >= 2) {
+    unsigned long long a, b, h;
+    memcpy(&a, &x, 8);
+    memcpy(&b, &y, 8);
+    h = (a * 0x9E3779B97F4A7C15ull) ^ (b + (kppref_pow_ulps == 2 ? 0x632BE59BD9B4E019ull
+                                                                  : 0xD1B54A32D192ED03ull));
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    if (h % 3 == 1) r = nextafter(r, HUGE_VAL);
+    if (h % 3 == 2) r = nextafter(r, -HUGE_VAL);
+  }
   return r;
 }
 

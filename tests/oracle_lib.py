@@ -237,8 +237,10 @@ def integrator_alternates(kind: str, mech: str, var, fix, temp, tstart, tend, at
     """VAR after the same SDIRK or Runge-Kutta integration by the reference
     under other valid last-ulp roundings: compiled with FMA contraction; SUN
     one ulp up and down at every evaluation; the integrator's pow() one ulp
-    up and down (the step-size factor and the Newton convergence tests decide
-    on it); Update_SUN's cos() one ulp up and down (SUN = (1 + cos)/2 cancels
+    up and down, and one ulp off in a direction that varies from call to call
+    (two hashes of the arguments: the step-size factor, the LU reuse test and
+    the Newton convergence tests decide on pow results, so per-call errors
+    can change the step sequence); Update_SUN's cos() one ulp up and down (SUN = (1 + cos)/2 cancels
     near sunrise and sunset, where a one-ulp cosine moves SUN far more than
     one ulp of SUN does)."""
     cls = SdirkOracle if kind == "sdirk" else RkOracle
@@ -252,8 +254,8 @@ def integrator_alternates(kind: str, mech: str, var, fix, temp, tstart, tend, at
         finally:
             o.set_sun_ulps(0)
     pw = cls(mech, "_pw")
-    for knob in (pw.set_pow_ulps, pw.set_cos_ulps):
-        for u in (1, -1):
+    for knob, values in ((pw.set_pow_ulps, (1, -1, 2, 3)), (pw.set_cos_ulps, (1, -1))):
+        for u in values:
             knob(u)
             try:
                 out.append(pw.integrate(*args, cfactor=cfactor, sun=sun)[0])
