@@ -12,6 +12,7 @@
 #   oracle/_ref/<mech>/libkppref_<mech>.so        -O (reference flags, util/Makefile_c:3)
 #   oracle/_ref/<mech>/libkppref_<mech>_O3.so     -O3 -march=x86-64-v3 (FMA contraction:
 #                                                 the same code with another valid rounding)
+#   oracle/_ref/<mech>/libkppref_<mech>_cs.so     Update_SUN's cos() one ulp on request
 #   oracle/_ref/<mech>_sdirk/libkppsd_<mech>[_O3|_pw].so  the model with the reference
 #                                                 SDIRK integrator (int/sdirk.c)
 #   oracle/_ref/<mech>_rk/libkpprk_<mech>[_O3|_pw].so  ... with the reference Runge-Kutta
@@ -57,10 +58,16 @@ done
 build_integrator_model() {
   local mech="$1" integ="$2" driver="$3" tag="$4" prefix="$5"
   local ds="$OUT/${mech}_${tag}"
+  local model="#MODEL      $mech"
   rm -rf "$ds"
   mkdir -p "$ds"
+  if [ "$mech" = "mcm_isoprene" ]; then
+    # the translated MCM (kpp_b200/gen/mcm.py), included after the SUN override
+    (cd "$HERE/.." && python -m kpp_b200.gen.mcm --home "$KPP_REF" --out "$ds" > /dev/null)
+    model=""
+  fi
   cat > "$ds/$mech.kpp" <<EOF
-#MODEL      $mech
+$model
 #LANGUAGE   C
 #DOUBLE     ON
 #INTEGRATOR $integ
@@ -79,6 +86,7 @@ build_integrator_model() {
   if (kppref_sun_ulps < 0) SUN = nextafter(SUN, -1.0);
 #ENDINLINE
 EOF
+  if [ "$mech" = "mcm_isoprene" ]; then echo "#INCLUDE    mcm_isoprene_c.eqn" >> "$ds/$mech.kpp"; fi
   (cd "$ds" && KPP_HOME="$KPP_REF" "$OUT/kpp" "$mech.kpp" > kpp.log 2>&1) || {
     echo "build_ref: kpp ($integ) failed for $mech" >&2; tail -20 "$ds/kpp.log" >&2; exit 1; }
   local srcs=() others=() f
@@ -165,8 +173,9 @@ EOF
   # the same model with the reference SDIRK (int/sdirk.c) and Runge-Kutta
   # (int/runge_kutta.c) integrators and their batch drivers, for those
   # entries' parity tests
+  build_integrator_model "$mech" sdirk batch_driver_sdirk sdirk kppsd
+  # (Runge-Kutta is built for mechanisms with LU_NONZERO < 2000: not MCM)
   if [ "$mech" != "mcm_isoprene" ]; then
-    build_integrator_model "$mech" sdirk batch_driver_sdirk sdirk kppsd
     build_integrator_model "$mech" runge_kutta batch_driver_rk rk kpprk
   fi
 done

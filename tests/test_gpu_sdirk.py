@@ -107,6 +107,16 @@ def test_sdirk_saprc99_matches_reference(method):
     check(got, ref, alt, f"saprc99 method {method}")
 
 
+@pytest.mark.parametrize("method", [1, 5])
+def test_sdirk_mcm_matches_reference(method):
+    from kpp_b200 import build
+    if not build.library_path("mcm_isoprene").exists():
+        pytest.skip("mcm_isoprene is built on request: python -m kpp_b200.build mcm_isoprene")
+    ic, rc = controls(method=method)
+    got, ref, alt = run_both("mcm_isoprene", 64, 7, ic, rc)
+    check(got, ref, alt, f"mcm method {method}")
+
+
 def _controls_cases():
     return [
         ("max_steps_3", dict(max_steps=3), {}),

@@ -18,7 +18,7 @@ import pytest
 from kpp_b200 import workloads
 from oracle_lib import REPO, OracleLib, SdirkOracle, _p, ensure_built, sdirk_lib_path
 
-MECHS = {"small_strato": 64, "saprc99": 16}
+MECHS = {"small_strato": 64, "saprc99": 16, "mcm_isoprene": 4}
 
 
 def _controls(method=3, scalar_tol=True, **kw):
@@ -87,6 +87,10 @@ def _host_integrate(lib, var, fix, temp, t0, t1, atol, rtol, ic, rc, cfactor, su
 def test_sdirk_restatement_bit_identical_to_reference(mech, tmp_path):
     if not sdirk_lib_path(mech).exists():
         pytest.skip("SDIRK oracle library not present")
+    if mech == "mcm_isoprene":
+        from kpp_b200 import build
+        if not build.library_path(mech).exists():
+            pytest.skip("mcm_isoprene is built on request")
     lib = _host_lib(mech, tmp_path)
     o = SdirkOracle(mech)
     ref = OracleLib(mech)
