@@ -106,8 +106,18 @@ EOF
   echo "build_ref: $mech ($integ) -> $ds/lib${prefix}_${mech}.so"
 }
 
+# A mechanism whose outputs were built from the same oracle sources (this
+# script, refkpp/, ros_oracle.c, the MCM translator) is left as it is.
+SRC_KEY="$(cat "$HERE/build_ref.sh" "$HERE"/refkpp/*.c "$HERE"/refkpp/*.h "$HERE/ros_oracle.c" \
+  "$HERE"/../kpp_b200/gen/mcm.py "$HERE"/../kpp_b200/gen/fortran.py | sha256sum | cut -d' ' -f1)"
+
 for mech in "${MECHS[@]}"; do
   d="$OUT/$mech"
+  if [ -f "$OUT/$mech.stamp" ] && [ "$(cat "$OUT/$mech.stamp")" = "$SRC_KEY" ]; then
+    echo "build_ref: $mech up to date"
+    continue
+  fi
+  rm -f "$OUT/$mech.stamp"
   rm -rf "$d"
   mkdir -p "$d"
   # The wrapper selects the C language, the reference Rosenbrock integrator and
@@ -178,4 +188,5 @@ EOF
   if [ "$mech" != "mcm_isoprene" ]; then
     build_integrator_model "$mech" runge_kutta batch_driver_rk rk kpprk
   fi
+  echo "$SRC_KEY" > "$OUT/$mech.stamp"
 done
