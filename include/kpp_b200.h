@@ -136,8 +136,8 @@ int kpp_b200_sdirk(int ncells, int ld, double *var, const double *fix,
  * no step taken.  The reference prints the errors it meets while integrating
  * and carries on; here a cell whose step size becomes 0 or NaN stops with
  * -10 and one that needs more than icntrl[3] + 200000 steps with -9 (the
- * reference would not return from either).  Mechanisms with LU_NONZERO <
- * 2000 only (KPP_B200_EINVAL otherwise).  Device pointers, asynchronous. */
+ * reference would not return from either).  Device pointers,
+ * asynchronous. */
 int kpp_b200_runge_kutta(int ncells, int ld, double *var, const double *fix,
                          const double *temp, const double *cfactor, const double *sun,
                          const double *tstart, const double *tend, const double *atol,

@@ -29,9 +29,10 @@
 #pragma once
 
 // Doubles of work storage one thread slot needs in the scratch layout: the
-// Jacobian and the three LU factors (E1, E2R, E2I), 18 vectors, rate
-// constants and the Fun / Jac_SP temporaries.
-constexpr long kRkPerSlot = 4L * LU_NZ + 18L * NVAR + 2L * NREACT + KPP_NJAC_TMP;
+// Jacobian and the three LU factors (E1, E2R, E2I), 18 vectors, the complex
+// LU's dense work row (two vectors, used by the generic form of large
+// mechanisms), rate constants and the Fun / Jac_SP temporaries.
+constexpr long kRkPerSlot = 4L * LU_NZ + 20L * NVAR + 2L * NREACT + KPP_NJAC_TMP;
 
 namespace rk {
 
@@ -351,12 +352,13 @@ inline Controls make_controls(const int* icntrl, const double* rcntrl) {
 // Per-cell work arrays: the Jacobian (kept for SkipJac), the real LU E1 and
 // the complex LU (E2R, E2I); Y, FO, SCAL, Z1..Z4, DZ1..DZ4, G, TMP, the
 // stage value F, the estimate's F2 and the interpolation polynomial CONT;
-// rate constants and the Fun / Jac_SP temporaries.
+// the complex LU's work row (WR, WI); rate constants and the Fun / Jac_SP
+// temporaries.
 constexpr long kPerSlot = kRkPerSlot;
 
 #if defined(KPP_SCRATCH)
 struct Work {
-  Strided y, fo, scal, z1, z2, z3, z4, dz1, dz2, dz3, dz4, g, tmp, f, f2, c0, c1, c2;
+  Strided y, fo, scal, z1, z2, z3, z4, dz1, dz2, dz3, dz4, g, tmp, f, f2, c0, c1, c2, wr, wi;
   Strided fjac, e1, e2r, e2i, rconst, a, b;
   __device__ __forceinline__ Work(double* base, long slot) {
     double* block = base + (slot / kLanes) * kPerSlot * kLanes + (slot % kLanes);
@@ -370,7 +372,7 @@ struct Work {
     z1 = take(NVAR); z2 = take(NVAR); z3 = take(NVAR); z4 = take(NVAR);
     dz1 = take(NVAR); dz2 = take(NVAR); dz3 = take(NVAR); dz4 = take(NVAR);
     g = take(NVAR); tmp = take(NVAR); f = take(NVAR); f2 = take(NVAR);
-    c0 = take(NVAR); c1 = take(NVAR); c2 = take(NVAR);
+    c0 = take(NVAR); c1 = take(NVAR); c2 = take(NVAR); wr = take(NVAR); wi = take(NVAR);
     fjac = take(LU_NZ); e1 = take(LU_NZ); e2r = take(LU_NZ); e2i = take(LU_NZ);
     rconst = take(NREACT); a = take(NREACT); b = take(KPP_NJAC_TMP);
   }
@@ -379,7 +381,7 @@ struct Work {
 struct Work {
   double y[NVAR], fo[NVAR], scal[NVAR], z1[NVAR], z2[NVAR], z3[NVAR], z4[NVAR];
   double dz1[NVAR], dz2[NVAR], dz3[NVAR], dz4[NVAR], g[NVAR], tmp[NVAR], f[NVAR], f2[NVAR];
-  double c0[NVAR], c1[NVAR], c2[NVAR];
+  double c0[NVAR], c1[NVAR], c2[NVAR], wr[NVAR], wi[NVAR];
   double fjac[LU_NZ], e1[LU_NZ], e2r[LU_NZ], e2i[LU_NZ];
   double rconst[NREACT > 0 ? NREACT : 1], a[NREACT > 0 ? NREACT : 1], b[KPP_NJAC_TMP];
   __device__ __forceinline__ Work(double*, long) {}
@@ -510,7 +512,11 @@ __device__ __forceinline__ int decomp(const Method& m, double h, W& w, Stats& st
   }
   kpp_add_diagonal(w.e2r, alpha_h);
   kpp_add_diagonal(w.e2i, beta_h);
+#if defined(KPP_CMPLX_GENERIC)
+  ising = kpp_decomp_cmplx_w(w.e2r, w.e2i, w.wr, w.wi);
+#else
   ising = kpp_decomp_cmplx(w.e2r, w.e2i);
+#endif
   st.ndec++;
   return ising;
 }

@@ -32,7 +32,7 @@
 #include "../../include/kpp_b200.h"
 #include "kpp_ratelaws.cuh"
 #include KPP_MECH_HEADER
-#if KPP_PART == 7 && KPP_LU_NONZERO < 2000
+#if KPP_PART == 7
 #include KPP_CMPLX_HEADER
 #endif
 
@@ -508,7 +508,6 @@ int launch_sdirk(LaunchArgs& a, int grid, cudaStream_t s) {
 #if KPP_PART == 7
 #include "kpp_rk.cuh"
 
-#if KPP_LU_NONZERO < 2000
 // One thread slot integrates cells slot, slot + nslots, ... with the C
 // RungeKutta (int/runge_kutta.c); the shared controls and the method table
 // come in `c`, RCNTRL in rpar of the launch.
@@ -548,12 +547,6 @@ int launch_rk(LaunchArgs& a, int grid, cudaStream_t s) {
   rk_kernel<<<grid, kBlock, 0, s>>>(a, c);
   return check_launch("rk_kernel");
 }
-#else
-int launch_rk(LaunchArgs&, int, cudaStream_t) {
-  return fail(KPP_B200_EINVAL,
-              "kpp_b200_runge_kutta: built for mechanisms with LU_NONZERO < 2000 only");
-}
-#endif
 #endif  // KPP_PART == 7
 
 #else  // KPP_PART == 0

@@ -13,7 +13,8 @@
 //                      (src/gen.c:1960-2034)
 // and a second header, <prefix>_cmplx.cuh, with the complex LU the
 // Runge-Kutta methods factorise (KppDecompCmplxR / KppSolveCmplxR of
-// util/sutil.c:28-90, unrolled in the same operation order).
+// util/sutil.c:28-90: unrolled in the same operation order, or for patterns
+// of 2000 entries or more the generic loops over the LU tables).
 //
 // Arithmetic is the reference's, operation for operation: expression trees
 // are built with the same constant folding (multiplying by a constant 1
@@ -878,7 +879,84 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   // performs the same operations on the same values.
   long ops_decomp_c = 0, ops_solve_c = 0;
   std::ostringstream oc;  // written to <prefix>_cmplx.cuh
-  {
+  if (m.lu_nonzero >= 2000) {
+    // Large patterns: the generic loops over the LU tables, with the dense
+    // work row of the reference (the unrolled form would take another long
+    // device compile); the same operations in the same order.
+    auto table = [&](const char* name, const std::vector<int>& v) {
+      oc << "__constant__ int " << name << "[" << v.size() << "] = {";
+      for (size_t i = 0; i < v.size(); i++) oc << (i % 16 == 0 ? "\n    " : " ") << v[i] << ",";
+      oc << "};\n";
+    };
+    oc << "#define KPP_CMPLX_GENERIC 1\n";
+    table("kpp_cx_crow", m.lu_crow);
+    table("kpp_cx_diag", m.lu_diag);
+    table("kpp_cx_icol", m.lu_icol);
+    for (int k = 0; k < nvar; k++)
+      for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+        const int j = m.lu_icol[kk];
+        ops_decomp_c += 11 + 8L * (m.lu_crow[j + 1] - m.lu_diag[j] - 1);
+      }
+    for (int i = 0; i < nvar; i++) ops_solve_c += 8L * (m.lu_crow[i + 1] - m.lu_crow[i] - 1) + 11;
+    oc << "\n"
+       "// In-place no-pivot sparse LU of the complex matrix (JR + i JI) of one cell,\n"
+       "// row by row through the dense work row (WR, WI) of NVAR entries; returns\n"
+       "// k+1 when the real or the imaginary part of row k's diagonal entry is zero\n"
+       "// on entry to its elimination, 0 on success.\n"
+       "template <class TJ, class TW>\n"
+       "__device__ __noinline__ int kpp_decomp_cmplx_w(TJ& JR, TJ& JI, TW& WR, TW& WI) {\n"
+       "  for (int k = 0; k < KPP_NVAR; k++) {\n"
+       "    const int dk = kpp_cx_diag[k], b = kpp_cx_crow[k], e = kpp_cx_crow[k + 1];\n"
+       "    if (JR[dk] == 0.0) return k + 1;\n"
+       "    if (JI[dk] == 0.0) return k + 1;\n"
+       "    for (int kk = b; kk < e; kk++) {\n"
+       "      WR[kpp_cx_icol[kk]] = JR[kk];\n"
+       "      WI[kpp_cx_icol[kk]] = JI[kk];\n"
+       "    }\n"
+       "    for (int kk = b; kk < dk; kk++) {\n"
+       "      const int j = kpp_cx_icol[kk], dj = kpp_cx_diag[j];\n"
+       "      const double den = JR[dj]*JR[dj] + JI[dj]*JI[dj];\n"
+       "      const double ar = -(WR[j]*JR[dj] + WI[j]*JI[dj])/den;\n"
+       "      const double ai = -(WI[j]*JR[dj] - WR[j]*JI[dj])/den;\n"
+       "      WR[j] = -ar;\n"
+       "      WI[j] = -ai;\n"
+       "      for (int jj = dj + 1; jj < kpp_cx_crow[j + 1]; jj++) {\n"
+       "        const int c = kpp_cx_icol[jj];\n"
+       "        WR[c] = WR[c] + ar*JR[jj] - ai*JI[jj];\n"
+       "        WI[c] = WI[c] + ar*JI[jj] + ai*JR[jj];\n"
+       "      }\n"
+       "    }\n"
+       "    for (int kk = b; kk < e; kk++) {\n"
+       "      JR[kk] = WR[kpp_cx_icol[kk]];\n"
+       "      JI[kk] = WI[kpp_cx_icol[kk]];\n"
+       "    }\n"
+       "  }\n"
+       "  return 0;\n"
+       "}\n\n"
+       "// Solve (LU) x = b in place for the complex LU of kpp_decomp_cmplx_w, b given\n"
+       "// in (XR, XI).\n"
+       "template <class TJ, class TX>\n"
+       "__device__ __noinline__ void kpp_solve_cmplx(const TJ& JR, const TJ& JI, TX& XR, TX& XI) {\n"
+       "  for (int i = 0; i < KPP_NVAR; i++)\n"
+       "    for (int j = kpp_cx_crow[i]; j < kpp_cx_diag[i]; j++) {\n"
+       "      const int c = kpp_cx_icol[j];\n"
+       "      XR[i] = XR[i] - (JR[j]*XR[c] - JI[j]*XI[c]);\n"
+       "      XI[i] = XI[i] - (JR[j]*XI[c] + JI[j]*XR[c]);\n"
+       "    }\n"
+       "  for (int i = KPP_NVAR - 1; i >= 0; i--) {\n"
+       "    const int d = kpp_cx_diag[i];\n"
+       "    double sumr = XR[i], sumi = XI[i];\n"
+       "    for (int j = d + 1; j < kpp_cx_crow[i + 1]; j++) {\n"
+       "      const int c = kpp_cx_icol[j];\n"
+       "      sumr = sumr - (JR[j]*XR[c] - JI[j]*XI[c]);\n"
+       "      sumi = sumi - (JR[j]*XI[c] + JI[j]*XR[c]);\n"
+       "    }\n"
+       "    const double den = JR[d]*JR[d] + JI[d]*JI[d];\n"
+       "    XR[i] = (sumr*JR[d] + sumi*JI[d])/den;\n"
+       "    XI[i] = (sumi*JR[d] - sumr*JI[d])/den;\n"
+       "  }\n"
+       "}\n\n";
+  } else {
     std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
     for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
     const bool chunked = m.lu_nonzero >= 2000;

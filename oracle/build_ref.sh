@@ -184,9 +184,6 @@ EOF
   # (int/runge_kutta.c) integrators and their batch drivers, for those
   # entries' parity tests
   build_integrator_model "$mech" sdirk batch_driver_sdirk sdirk kppsd
-  # (Runge-Kutta is built for mechanisms with LU_NONZERO < 2000: not MCM)
-  if [ "$mech" != "mcm_isoprene" ]; then
-    build_integrator_model "$mech" runge_kutta batch_driver_rk rk kpprk
-  fi
+  build_integrator_model "$mech" runge_kutta batch_driver_rk rk kpprk
   echo "$SRC_KEY" > "$OUT/$mech.stamp"
 done

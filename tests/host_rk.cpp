@@ -40,7 +40,14 @@ using namespace kpp_b200_impl;
 
 extern "C" {
 
-int host_decomp_cmplx(double* jr, double* ji) { return kpp_decomp_cmplx(jr, ji); }
+int host_decomp_cmplx(double* jr, double* ji) {
+#if defined(KPP_CMPLX_GENERIC)
+  double wr[KPP_NVAR], wi[KPP_NVAR];
+  return kpp_decomp_cmplx_w(jr, ji, wr, wi);
+#else
+  return kpp_decomp_cmplx(jr, ji);
+#endif
+}
 
 void host_solve_cmplx(const double* jr, const double* ji, double* xr, double* xi) {
   kpp_solve_cmplx(jr, ji, xr, xi);

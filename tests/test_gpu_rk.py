@@ -218,17 +218,12 @@ def test_rk_empty_and_ragged_batches():
     assert torch.all(r.ierr[:37] == 1)
 
 
-def test_rk_not_built_for_large_mechanisms_reports_error():
-    """Mechanisms with LU_NONZERO >= 2000 (MCM) have no Runge-Kutta kernel:
-    the entry returns KPP_B200_EINVAL with a message, without a launch."""
-    from kpp_b200 import build, load
+@pytest.mark.parametrize("method", [0, 3])
+def test_rk_mcm_matches_reference(method):
+    """MCM (LU_NONZERO 7123) factorises with the generic complex LU."""
+    from kpp_b200 import build
     if not build.library_path("mcm_isoprene").exists():
-        pytest.skip("mcm_isoprene is built on request")
-    m = load("mcm_isoprene")
-    assert m.lu_nonzero >= 2000
-    ic, rc = rk_controls(method=0)
-    n = 32
-    d = lambda *s: torch.ones(*s, dtype=torch.float64, device="cuda")
-    with pytest.raises(RuntimeError, match="LU_NONZERO"):
-        m.runge_kutta(d(m.nvar, n), d(max(m.nfix, 1), n), d(n), d(n) * 0, d(n), d(1), d(1) * 1e-3,
-                      ic, rc)
+        pytest.skip("mcm_isoprene is built on request: python -m kpp_b200.build mcm_isoprene")
+    ic, rc = rk_controls(method=method)
+    got, ref, alt, atol, rtol = run_both("mcm_isoprene", 64, 7, ic, rc)
+    check(got, ref, alt, f"mcm method {method}", atol, rtol)

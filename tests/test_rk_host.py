@@ -69,7 +69,8 @@ CASES = ([(f"method_{m}_sdirk_err_{e}", dict(method=m, sdirk_error=e), None)
     ("tiny_rtol", dict(), "tiny_rtol"),
 ])
 
-MECHS = {"small_strato": (64, (0, 3), None), "saprc99": (8, (0,), "methods")}
+MECHS = {"small_strato": (64, (0, 3), None), "saprc99": (8, (0,), "methods"),
+         "mcm_isoprene": (4, (0,), "methods")}
 
 
 def _host_lib(mech, tmp_path):
