@@ -959,71 +959,36 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   } else {
     std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
     for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
-    const bool chunked = m.lu_nonzero >= 2000;
-    const int kChunkOps = 1200;
-    std::vector<int> starts = {0};
-    if (chunked) {
-      int acc = 0;
-      for (int k = 0; k < nvar; k++) {
-        int row_ops = 0;
-        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
-          int j = m.lu_icol[kk];
-          row_ops += 1 + 2 * (m.lu_crow[j + 1] - m.lu_diag[j] - 1);
-        }
-        if (acc > 0 && acc + row_ops > kChunkOps) {
-          starts.push_back(k);
-          acc = 0;
-        }
-        acc += row_ops;
-      }
-    }
-    starts.push_back(nvar);
-    const int nchunks = (int)starts.size() - 1;
-    const char* head =
-        "// In-place no-pivot sparse LU of the complex matrix (JR + i JI) of one cell;\n"
-        "// returns k+1 when the real or the imaginary part of row k's diagonal entry\n"
-        "// is zero on entry to its elimination, 0 on success.\n";
-    for (int c = 0; c < nchunks; c++) {
-      if (nchunks > 1)
-        oc << "// Rows " << starts[c] << ".." << starts[c + 1] - 1 << " of the complex LU.\n"
-          << "template <class TJ>\n"
-          << "__device__ __noinline__ int kpp_decomp_cmplx_rows" << c << "(TJ& JR, TJ& JI) {\n";
-      else
-        oc << head << "template <class TJ>\n"
-          << "__device__ KPP_MECH_INLINE int kpp_decomp_cmplx(TJ& JR, TJ& JI) {\n";
-      oc << "  double ar, ai, den;\n";
-      for (int k = starts[c]; k < starts[c + 1]; k++) {
-        const int dk = m.lu_diag[k];
-        oc << "  if (JR[" << dk << "] == 0.0) return " << (k + 1) << ";\n"
-          << "  if (JI[" << dk << "] == 0.0) return " << (k + 1) << ";\n";
-        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
-          const int j = m.lu_icol[kk], dj = m.lu_diag[j];
-          ops_decomp_c += 3 + 8;
-          oc << "  den = JR[" << dj << "]*JR[" << dj << "] + JI[" << dj << "]*JI[" << dj << "];\n"
-            << "  ar = -(JR[" << kk << "]*JR[" << dj << "] + JI[" << kk << "]*JI[" << dj
-            << "])/den;\n"
-            << "  ai = -(JI[" << kk << "]*JR[" << dj << "] - JR[" << kk << "]*JI[" << dj
-            << "])/den;\n"
-            << "  JR[" << kk << "] = -ar;\n  JI[" << kk << "] = -ai;\n";
-          for (int jj = dj + 1; jj < m.lu_crow[j + 1]; jj++) {
-            const int t = pos[k][m.lu_icol[jj]];
-            ops_decomp_c += 8;
-            oc << "  JR[" << t << "] = JR[" << t << "] + ar*JR[" << jj << "] - ai*JI[" << jj
-              << "];\n"
-              << "  JI[" << t << "] = JI[" << t << "] + ar*JI[" << jj << "] + ai*JR[" << jj
-              << "];\n";
-          }
+    oc << "// In-place no-pivot sparse LU of the complex matrix (JR + i JI) of one cell;\n"
+          "// returns k+1 when the real or the imaginary part of row k's diagonal entry\n"
+          "// is zero on entry to its elimination, 0 on success.\n"
+          "template <class TJ>\n"
+          "__device__ KPP_MECH_INLINE int kpp_decomp_cmplx(TJ& JR, TJ& JI) {\n"
+          "  double ar, ai, den;\n";
+    for (int k = 0; k < nvar; k++) {
+      const int dk = m.lu_diag[k];
+      oc << "  if (JR[" << dk << "] == 0.0) return " << (k + 1) << ";\n"
+         << "  if (JI[" << dk << "] == 0.0) return " << (k + 1) << ";\n";
+      for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+        const int j = m.lu_icol[kk], dj = m.lu_diag[j];
+        ops_decomp_c += 3 + 8;
+        oc << "  den = JR[" << dj << "]*JR[" << dj << "] + JI[" << dj << "]*JI[" << dj << "];\n"
+           << "  ar = -(JR[" << kk << "]*JR[" << dj << "] + JI[" << kk << "]*JI[" << dj
+           << "])/den;\n"
+           << "  ai = -(JI[" << kk << "]*JR[" << dj << "] - JR[" << kk << "]*JI[" << dj
+           << "])/den;\n"
+           << "  JR[" << kk << "] = -ar;\n  JI[" << kk << "] = -ai;\n";
+        for (int jj = dj + 1; jj < m.lu_crow[j + 1]; jj++) {
+          const int t = pos[k][m.lu_icol[jj]];
+          ops_decomp_c += 8;
+          oc << "  JR[" << t << "] = JR[" << t << "] + ar*JR[" << jj << "] - ai*JI[" << jj
+             << "];\n"
+             << "  JI[" << t << "] = JI[" << t << "] + ar*JI[" << jj << "] + ai*JR[" << jj
+             << "];\n";
         }
       }
-      oc << "  (void)ar; (void)ai; (void)den;\n  return 0;\n}\n\n";
     }
-    if (nchunks > 1) {
-      oc << head << "template <class TJ>\n"
-        << "__device__ KPP_MECH_INLINE int kpp_decomp_cmplx(TJ& JR, TJ& JI) {\n  int r;\n";
-      for (int c = 0; c < nchunks; c++)
-        oc << "  if ((r = kpp_decomp_cmplx_rows" << c << "(JR, JI)) != 0) return r;\n";
-      oc << "  return 0;\n}\n\n";
-    }
+    oc << "  (void)ar; (void)ai; (void)den;\n  return 0;\n}\n\n";
 
     oc << "// Solve (LU) x = b in place for the complex LU of kpp_decomp_cmplx, b given\n"
          "// in (XR, XI).\n"
