@@ -144,6 +144,23 @@ int kpp_b200_runge_kutta(int ncells, int ld, double *var, const double *fix,
                          const double *rtol, const int *icntrl, const double *rcntrl,
                          int *istatus, double *rstatus, int *ierr, void *stream);
 
+/* kpp_b200_sdirk and kpp_b200_runge_kutta on HOST arrays, for a host model
+ * that keeps its cells in host memory as the reference's INTEGRATE does
+ * (int/sdirk.c:92-166, int/runge_kutta.c:114-198): chunks of `chunk` cells
+ * (0: 2^18) are copied in, integrated and copied back on two alternating
+ * streams, so copies overlap the integration; synchronous.  Same arguments
+ * and results as the device entries; pinned host memory gives full overlap. */
+int kpp_b200_sdirk_host(int ncells, int ld, double *var, const double *fix,
+                        const double *temp, const double *cfactor, const double *sun,
+                        const double *tstart, const double *tend, const double *atol,
+                        const double *rtol, const int *icntrl, const double *rcntrl,
+                        int *istatus, double *rstatus, int *ierr, int chunk);
+int kpp_b200_runge_kutta_host(int ncells, int ld, double *var, const double *fix,
+                              const double *temp, const double *cfactor, const double *sun,
+                              const double *tstart, const double *tend, const double *atol,
+                              const double *rtol, const int *icntrl, const double *rcntrl,
+                              int *istatus, double *rstatus, int *ierr, int chunk);
+
 /* The host model's time loop (drv/general.c:59-76) over INTEGRATE
  * (int/rosenbrock.c:94-133) for every cell in one persistent launch: each cell
  * makes ncalls consecutive calls Rosenbrock(T, T + dt) with T = tstart[c]

@@ -912,7 +912,7 @@ struct ChunkBuffers {
         {(void**)&var, (size_t)NVAR * n * d}, {(void**)&fix, (size_t)(NFIX_TRUE > 0 ? NFIX_TRUE : 1) * n * d},
         {(void**)&temp, n * d}, {(void**)&cfactor, n * d}, {(void**)&sun, n * d},
         {(void**)&tstart, n * d}, {(void**)&tend, n * d}, {(void**)&hstart, n * d},
-        {(void**)&rstatus, 2 * n * d}, {(void**)&atol, NVAR * d}, {(void**)&rtol, NVAR * d},
+        {(void**)&rstatus, 3 * n * d}, {(void**)&atol, NVAR * d}, {(void**)&rtol, NVAR * d},
         {(void**)&istatus, 8 * n * sizeof(int)}, {(void**)&ierr, n * sizeof(int)}};
     for (auto& w : want) {
       cudaError_t e = cudaMalloc(w.p, w.bytes);
@@ -937,11 +937,14 @@ inline cudaError_t copy_rows(void* dst, long dld, const void* src, long sld, lon
   return cudaMemcpy2DAsync(dp, dld * elem, sp, sld * elem, cols * elem, rows, kind, s);
 }
 
+// The host-array entries: chunks of cells copied in, integrated and copied
+// out on two alternating streams.  `which`: 0 Rosenbrock (rstatus 2 rows), 1
+// SDIRK, 2 Runge-Kutta (3 rows; no hstart).
 int host_pipeline(int ncells, int ld, double* var, const double* fix, const double* temp,
                   const double* cfactor, const double* sun, const double* tstart,
                   const double* tend, const double* atol, const double* rtol, const int* ipar,
                   const double* rpar, const double* hstart, int* istatus, double* rstatus,
-                  int* ierr, int chunk) {
+                  int* ierr, int chunk, int which) {
   static std::mutex mu;
   static std::map<int, ChunkBuffers[2]> per_device;
   std::lock_guard<std::mutex> lock(mu);  // one host pipeline per process at a time
@@ -987,15 +990,28 @@ int host_pipeline(int ncells, int ld, double* var, const double* fix, const doub
               sun ? B.sun : nullptr, B.tstart, B.tend, B.atol, B.rtol, ipar, rpar,
               hstart ? B.hstart : nullptr, B.istatus, B.rstatus, B.ierr);
     a.nslots = slots_for((int)n);
-    int rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
-    if (rc != KPP_B200_OK) return rc;
-    a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
-    rc = launch_rosenbrock(a, s);
+    int rc;
+    if (which == 0) {
+      rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+      if (rc != KPP_B200_OK) return rc;
+      a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+      rc = launch_rosenbrock(a, s);
+    } else {
+      const long per = which == 1 ? kSdirkPerSlot : kRkPerSlot;
+      const size_t bytes =
+          kUsesScratch ? (size_t)per * (size_t)kSlotStride * sizeof(double) : 0;
+      rc = cached_scratch(s, bytes, &a.scratch);
+      if (rc != KPP_B200_OK) return rc;
+      a.scratch_doubles = bytes / sizeof(double);
+      rc = which == 1 ? launch_sdirk(a, (int)(a.nslots / kBlock), s)
+                      : launch_rk(a, (int)(a.nslots / kBlock), s);
+    }
     if (rc != KPP_B200_OK) return rc;
 
+    const long rst_rows = which == 0 ? 2 : 3;
     e = copy_rows(var, ld, B.var, csz, c0, n, NVAR, sizeof(double), D2H, s, false);
     if (e == cudaSuccess) e = copy_rows(istatus, ld, B.istatus, csz, c0, n, 8, sizeof(int), D2H, s, false);
-    if (e == cudaSuccess) e = copy_rows(rstatus, ld, B.rstatus, csz, c0, n, 2, sizeof(double), D2H, s, false);
+    if (e == cudaSuccess) e = copy_rows(rstatus, ld, B.rstatus, csz, c0, n, rst_rows, sizeof(double), D2H, s, false);
     if (e == cudaSuccess) e = copy_rows(ierr, ld, B.ierr, csz, c0, n, 1, sizeof(int), D2H, s, false);
     if (e != cudaSuccess) return cuda_fail("device->host copy", e);
   }
@@ -1262,7 +1278,33 @@ int kpp_b200_rosenbrock_host(int ncells, int ld, double* var, const double* fix,
                      ipar, rpar, hstart, istatus, rstatus, ierr);
   if (rc != KPP_B200_OK || ncells == 0) return rc;
   return host_pipeline(ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, ipar,
-                       rpar, hstart, istatus, rstatus, ierr, chunk);
+                       rpar, hstart, istatus, rstatus, ierr, chunk, 0);
+}
+
+int kpp_b200_sdirk_host(int ncells, int ld, double* var, const double* fix, const double* temp,
+                        const double* cfactor, const double* sun, const double* tstart,
+                        const double* tend, const double* atol, const double* rtol,
+                        const int* icntrl, const double* rcntrl, int* istatus, double* rstatus,
+                        int* ierr, int chunk) {
+  LaunchArgs chk;
+  int rc = fill_args(chk, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol,
+                     icntrl, rcntrl, nullptr, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  return host_pipeline(ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, icntrl,
+                       rcntrl, nullptr, istatus, rstatus, ierr, chunk, 1);
+}
+
+int kpp_b200_runge_kutta_host(int ncells, int ld, double* var, const double* fix,
+                              const double* temp, const double* cfactor, const double* sun,
+                              const double* tstart, const double* tend, const double* atol,
+                              const double* rtol, const int* icntrl, const double* rcntrl,
+                              int* istatus, double* rstatus, int* ierr, int chunk) {
+  LaunchArgs chk;
+  int rc = fill_args(chk, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol,
+                     icntrl, rcntrl, nullptr, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK || ncells == 0) return rc;
+  return host_pipeline(ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol, icntrl,
+                       rcntrl, nullptr, istatus, rstatus, ierr, chunk, 2);
 }
 
 int kpp_b200_fun_jac(int ncells, int ld, const double* var, const double* fix,

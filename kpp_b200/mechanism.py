@@ -98,6 +98,8 @@ class Mechanism:
                                      + [ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double)] + [_vp] * 4)
         L.kpp_b200_runge_kutta.argtypes = L.kpp_b200_sdirk.argtypes
+        L.kpp_b200_sdirk_host.argtypes = L.kpp_b200_sdirk.argtypes[:-1] + [ctypes.c_int]
+        L.kpp_b200_runge_kutta_host.argtypes = L.kpp_b200_sdirk_host.argtypes
         L.kpp_b200_user_species.argtypes = [_vp, _vp]
         L.kpp_b200_shuffle_user2kpp.argtypes = [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                 _vp, _vp]
@@ -353,6 +355,44 @@ class Mechanism:
             n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
             _ptr(tend), _ptr(atol), _ptr(rtol), ip, rp, _ptr(hstart), _ptr(out.istatus),
             _ptr(out.rstatus), _ptr(out.ierr), int(chunk)))
+        return out
+
+    def sdirk_host(self, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                   cfactor=None, sun=None, ncells=None, out=None,
+                   chunk: int = 0) -> RosenbrockResult:
+        """kpp_b200_sdirk on host tensors (kpp_b200_sdirk_host); synchronous."""
+        return self._integrator_host(self.lib.kpp_b200_sdirk_host, var, fix, temp, tstart,
+                                     tend, atol, rtol, icntrl, rcntrl, cfactor, sun, ncells,
+                                     out, chunk)
+
+    def runge_kutta_host(self, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                         cfactor=None, sun=None, ncells=None, out=None,
+                         chunk: int = 0) -> RosenbrockResult:
+        """kpp_b200_runge_kutta on host tensors (kpp_b200_runge_kutta_host);
+        synchronous."""
+        return self._integrator_host(self.lib.kpp_b200_runge_kutta_host, var, fix, temp,
+                                     tstart, tend, atol, rtol, icntrl, rcntrl, cfactor, sun,
+                                     ncells, out, chunk)
+
+    def _integrator_host(self, entry, var, fix, temp, tstart, tend, atol, rtol, icntrl, rcntrl,
+                         cfactor, sun, ncells, out, chunk):
+        f64, i32 = torch.float64, torch.int32
+        self._host(var, f64, "var")
+        ld = var.shape[1]
+        n = ld if ncells is None else ncells
+        for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                      (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun")):
+            self._host(t, f64, nm)
+        if out is None:
+            pin = torch.cuda.is_available()
+            out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, pin_memory=pin),
+                                   istatus=torch.empty(8, ld, dtype=i32, pin_memory=pin),
+                                   rstatus=torch.empty(3, ld, dtype=f64, pin_memory=pin))
+        ic = (ctypes.c_int * 20)(*[int(x) for x in icntrl])
+        rc = (ctypes.c_double * 20)(*[float(x) for x in rcntrl])
+        self._check(entry(n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun),
+                          _ptr(tstart), _ptr(tend), _ptr(atol), _ptr(rtol), ic, rc,
+                          _ptr(out.istatus), _ptr(out.rstatus), _ptr(out.ierr), int(chunk)))
         return out
 
     def fun_jac(self, var, fix, temp, time: float, cfactor=None, sun=None,

@@ -102,6 +102,14 @@ def test_entry_points_reject_bad_arguments_without_gpu():
     assert rc == 1 and b"null" in lib.kpp_b200_last_error()
     assert lib.kpp_b200_runge_kutta(0, 0, None, None, None, None, None, None, None, None, None,
                                     ip, rp, None, None, None, None) == 0
+    # and the host-array entries of both
+    for entry in (lib.kpp_b200_sdirk_host, lib.kpp_b200_runge_kutta_host):
+        rc = entry(4, 2, None, None, None, None, None, None, None, None, None, ip, rp, None, None,
+                   None, 0)
+        assert rc == 1 and b"ncells" in lib.kpp_b200_last_error()
+        rc = entry(4, 4, None, None, None, None, None, None, None, None, None, ip, rp, None, None,
+                   None, 0)
+        assert rc == 1 and b"null" in lib.kpp_b200_last_error()
 
 
 def test_controls_layouts():

@@ -214,3 +214,34 @@ def test_sdirk_cell_results_independent_of_batch(mech, ncells, newton_maxit):
         np.testing.assert_array_equal(a, b)
         np.testing.assert_array_equal(a[..., sub], c)
     assert full[1][4].sum() > 0  # rejected steps: the path was taken
+
+
+@pytest.mark.parametrize("mech,ncells", [("small_strato", 1000), ("saprc99", 600)])
+def test_sdirk_host_entry_matches_device_entry(mech, ncells):
+    """kpp_b200_sdirk_host (host arrays, chunks of 256 cells: several chunks
+    and a ragged last one; ld > ncells) gives the device entry's results bit
+    for bit."""
+    from kpp_b200 import load
+    m = load(mech)
+    wl = workloads.for_mechanism(m, mech, ncells, seed=4)
+    ic, rc = controls(method=3)
+    t0, t1 = wl.step_bounds(0)
+    var = dev(wl.var)
+    cf = None if wl.cfactor is None else dev(wl.cfactor)
+    sun = None if wl.sun is None else dev(wl.sun)
+    r = m.sdirk(var, dev(wl.fix), dev(wl.temp), dev(t0), dev(t1), dev(wl.atol), dev(wl.rtol), ic,
+                rc, cfactor=cf, sun=sun)
+    torch.cuda.synchronize()
+    ld = ncells + 24
+    pad = lambda a: torch.from_numpy(np.ascontiguousarray(np.concatenate(
+        [a, np.ones(a.shape[:-1] + (ld - ncells,))], axis=-1))).pin_memory()
+    hvar = pad(wl.var)
+    hr = m.sdirk_host(hvar, pad(wl.fix), pad(wl.temp), pad(t0), pad(t1),
+                      torch.from_numpy(wl.atol), torch.from_numpy(wl.rtol), ic, rc,
+                      cfactor=None if wl.cfactor is None else pad(wl.cfactor),
+                      sun=None if wl.sun is None else pad(wl.sun), ncells=ncells, chunk=256)
+    np.testing.assert_array_equal(hvar[:, :ncells].numpy(), var.cpu().numpy())
+    np.testing.assert_array_equal(hr.istatus[:, :ncells].numpy(), r.istatus.cpu().numpy())
+    np.testing.assert_array_equal(hr.rstatus[:, :ncells].numpy(), r.rstatus.cpu().numpy())
+    np.testing.assert_array_equal(hr.ierr[:ncells].numpy(), r.ierr.cpu().numpy())
+    assert torch.all(hvar[:, ncells:] == 1.0)
