@@ -10,7 +10,13 @@ kpp_b200/workloads.py), as the headline metric is quoted:
                 initial state with the default starting step (STEPMIN = 0),
                 the case a learned starting step and cost binning address;
   --mode chain  the cells' state carries over from step to step and each step
-                warm-starts from the previous step's Hexit, as INTEGRATE does.
+                warm-starts from the previous step's Hexit, as INTEGRATE does;
+  --mode diurnal  24 chained steps of cells of uneven stiffness, one launch per
+                step against one persistent work-queue launch;
+  --mode sdirk / --mode rk  the same fresh batch with the reference's other C
+                integrators (int/sdirk.c, --sdirk-method; int/runge_kutta.c,
+                --rk-method), their reference arms timing the reference's own
+                SDIRK / RungeKutta.
 
 Arms
   --impl kpp_b200   (default) the CUDA path.  `value` is device-timed with
