@@ -263,6 +263,18 @@ int kpp_b200_fun_jac(int ncells, int ld, const double *var, const double *fix,
                      const double *sun, double time, double *rconst,
                      double *vdot, double *jvs, void *stream);
 
+/* The building blocks of the discrete adjoint (int/rosenbrock_adj.c), for
+ * every cell: out = J uv (transposed = 0, Jac_SP_Vec) or out = J^T uv
+ * (transposed = 1, JacTR_SP_Vec), src/gen.c:1763-1880, with jvs
+ * [LU_NONZERO][ld] in the LU pattern, uv and out [NVAR][ld] (out must not be
+ * uv); and the solve of (LU)^T xx = x for a factorised jvs (KppSolveTR,
+ * src/gen.c:2036-2120; xx may be x).  Same operations in the same order as
+ * the generated C functions.  Device pointers, asynchronous. */
+int kpp_b200_jac_vec(int ncells, int ld, const double *jvs, const double *uv,
+                     double *out, int transposed, void *stream);
+int kpp_b200_solve_tr(int ncells, int ld, const double *jvs, const double *x,
+                      double *xx, void *stream);
+
 /* Batched no-pivot sparse LU (KppDecomp, util/sutil.c:2-23) of jvs
  * [LU_NONZERO][ld] in place, then one solve (KppSolve, src/gen.c:1960-2034)
  * of x [NVAR][ld] in place when x is not NULL.  ising[ld] receives the

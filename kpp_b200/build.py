@@ -175,6 +175,8 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> 
         f = ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT)]
         if part == 0 and host_header.exists():
             f.append(f'-DKPP_HOST_HEADER="{host_header}"')
+        if part == 0:
+            f.append(f'-DKPP_ADJ_HEADER="{header.with_name(header.stem + "_adj.cuh")}"')
         if part == RK_PART:
             f.append(f'-DKPP_CMPLX_HEADER="{header.with_name(header.stem + "_cmplx.cuh")}"')
         return f

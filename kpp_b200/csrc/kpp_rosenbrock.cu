@@ -35,6 +35,9 @@
 #if KPP_PART == 7
 #include KPP_CMPLX_HEADER
 #endif
+#if KPP_PART == 0
+#include KPP_ADJ_HEADER
+#endif
 
 // Translation-unit split (the build compiles this file once per part, in
 // parallel): KPP_PART 1..5 holds the kernel of Rosenbrock method 1..5 and its
@@ -657,6 +660,33 @@ __global__ void __launch_bounds__(128) decomp_solve_kernel(int ncells, int ld, d
     StridedLd x{x_g + cell, ld};
     kpp_solve(jvs, x);
   }
+}
+
+// The building blocks of the discrete adjoint, one cell per thread on the
+// [n][ld] arrays: J uv or J^T uv (Jac_SP_Vec / JacTR_SP_Vec) and the
+// transposed LU solve (KppSolveTR).
+__global__ void __launch_bounds__(128) jac_vec_kernel(int ncells, int ld, const double* jvs_g,
+                                                      const double* uv_g, double* out_g,
+                                                      int transposed) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= ncells) return;
+  const StridedLd jvs{const_cast<double*>(jvs_g) + cell, ld};
+  const StridedLd uv{const_cast<double*>(uv_g) + cell, ld};
+  StridedLd out{out_g + cell, ld};
+  if (transposed)
+    kpp_jactr_sp_vec(jvs, uv, out);
+  else
+    kpp_jac_sp_vec(jvs, uv, out);
+}
+
+__global__ void __launch_bounds__(128) solve_tr_kernel(int ncells, int ld, const double* jvs_g,
+                                                       const double* x_g, double* xx_g) {
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= ncells) return;
+  const StridedLd jvs{const_cast<double*>(jvs_g) + cell, ld};
+  const StridedLd x{const_cast<double*>(x_g) + cell, ld};
+  StridedLd xx{xx_g + cell, ld};
+  kpp_solve_tr(jvs, x, xx);
 }
 
 
@@ -1329,6 +1359,27 @@ int kpp_b200_decomp_solve(int ncells, int ld, double* jvs, double* x, int* ising
   decomp_solve_kernel<<<(ncells + kBlock - 1) / kBlock, kBlock, 0, (cudaStream_t)stream>>>(
       ncells, ld, jvs, x, ising);
   return check_launch("decomp_solve_kernel");
+}
+
+int kpp_b200_jac_vec(int ncells, int ld, const double* jvs, const double* uv, double* out,
+                     int transposed, void* stream) {
+  if (ncells < 0 || ld < ncells) return fail(KPP_B200_EINVAL, "need 0 <= ncells <= ld");
+  if (ncells == 0) return KPP_B200_OK;
+  if (!jvs || !uv || !out) return fail(KPP_B200_EINVAL, "null argument");
+  if (uv == out) return fail(KPP_B200_EINVAL, "out must not be uv");
+  jac_vec_kernel<<<(ncells + kBlock - 1) / kBlock, kBlock, 0, (cudaStream_t)stream>>>(
+      ncells, ld, jvs, uv, out, transposed);
+  return check_launch("jac_vec_kernel");
+}
+
+int kpp_b200_solve_tr(int ncells, int ld, const double* jvs, const double* x, double* xx,
+                      void* stream) {
+  if (ncells < 0 || ld < ncells) return fail(KPP_B200_EINVAL, "need 0 <= ncells <= ld");
+  if (ncells == 0) return KPP_B200_OK;
+  if (!jvs || !x || !xx) return fail(KPP_B200_EINVAL, "null argument");
+  solve_tr_kernel<<<(ncells + kBlock - 1) / kBlock, kBlock, 0, (cudaStream_t)stream>>>(
+      ncells, ld, jvs, x, xx);
+  return check_launch("solve_tr_kernel");
 }
 
 const char* kpp_b200_last_error(void) { return g_last_error; }

@@ -1042,6 +1042,81 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   if (!f) return false;
   // The complex LU lives in a header of its own, included after the main one
   // only by the integrators that need it (the Runge-Kutta methods).
+  // ---- Jac_SP_Vec, JacTR_SP_Vec, KppSolveTR (src/gen.c:1763-1880,2036-2120):
+  // the Jacobian (LU pattern) times a vector, its transpose times a vector,
+  // and the transposed LU solve; the building blocks of the discrete
+  // adjoint.  Terms are the Jacobian's structural entries (the diagonal
+  // always counts), summed in the generator's order.
+  std::ostringstream oa;
+  {
+    auto js = [&](int r, int c) { return r == c || m.jstruct[r][c]; };
+    std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
+    for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
+    oa << "// Generated by kppcu: the Jacobian-vector products and the transposed LU\n"
+          "// solve of the mechanism.  Include after the mechanism header.\n#pragma once\n\n"
+          "// JUV = J UV, J in the LU pattern (JVS).\n"
+          "template <class TJ, class TU, class TO>\n"
+          "__device__ KPP_MECH_INLINE void kpp_jac_sp_vec(const TJ& JVS, const TU& UV, TO& JUV) {\n";
+    for (int i = 0; i < nvar; i++) {
+      P sum = cnst(0);
+      for (int k = m.lu_crow[i]; k < m.lu_crow[i + 1]; k++)
+        if (js(i, m.lu_icol[k]))
+          sum = add(sum, mul(leaf("JVS[" + std::to_string(k) + "]"),
+                             leaf("UV[" + std::to_string(m.lu_icol[k]) + "]")));
+      oa << "  JUV[" << i << "] = " << print(sum) << ";\n";
+    }
+    oa << "}\n\n"
+          "// JTUV = J^T UV, J in the LU pattern (JVS).\n"
+          "template <class TJ, class TU, class TO>\n"
+          "__device__ KPP_MECH_INLINE void kpp_jactr_sp_vec(const TJ& JVS, const TU& UV, TO& JTUV) {\n";
+    for (int i = 0; i < nvar; i++) {
+      P sum = cnst(0);
+      for (int j = 0; j < nvar; j++)
+        if (js(j, i))
+          sum = add(sum, mul(leaf("JVS[" + std::to_string(pos[j][i]) + "]"),
+                             leaf("UV[" + std::to_string(j) + "]")));
+      oa << "  JTUV[" << i << "] = " << print(sum) << ";\n";
+    }
+    oa << "}\n\n"
+          "// Solve (LU)^T XX = X for the factorised JVS.\n"
+          "template <class TJ, class TX, class TY>\n"
+          "__device__ KPP_MECH_INLINE void kpp_solve_tr(const TJ& JVS, const TX& X, TY& XX) {\n";
+    // pos_t[c][r]: the LU entry (r, c), r != c, and the diagonal
+    std::vector<std::vector<int>> pos_t(nvar, std::vector<int>(nvar, -1));
+    for (int r = 0; r < nvar; r++) {
+      for (int k = m.lu_crow[r]; k < m.lu_crow[r + 1]; k++)
+        if (m.lu_icol[k] != r) pos_t[m.lu_icol[k]][r] = k;
+      pos_t[r][r] = m.lu_diag[r];
+    }
+    for (int i = 0; i < nvar; i++) {
+      P sum = leaf("X[" + std::to_string(i) + "]");
+      for (int j = 0; j < i; j++)
+        if (pos_t[i][j] >= 0)
+          sum = sub(sum, mul(leaf("JVS[" + std::to_string(pos_t[i][j]) + "]"),
+                             leaf("XX[" + std::to_string(j) + "]")));
+      sum = divide(sum, leaf("JVS[" + std::to_string(m.lu_diag[i]) + "]"));
+      oa << "  XX[" << i << "] = " << print(sum) << ";\n";
+    }
+    for (int i = nvar - 1; i >= 0; i--) {
+      P sum = leaf("XX[" + std::to_string(i) + "]");
+      bool any = false;
+      for (int j = i + 1; j < nvar; j++)
+        if (pos_t[i][j] >= 0) {
+          sum = sub(sum, mul(leaf("JVS[" + std::to_string(pos_t[i][j]) + "]"),
+                             leaf("XX[" + std::to_string(j) + "]")));
+          any = true;
+        }
+      if (any) oa << "  XX[" << i << "] = " << print(sum) << ";\n";
+    }
+    oa << "}\n";
+  }
+  {
+    std::ofstream fa(out_prefix + "_adj.cuh");
+    if (!fa) return false;
+    fa << oa.str();
+    if (!fa) return false;
+  }
+
   std::ofstream fc(out_prefix + "_cmplx.cuh");
   if (!fc) return false;
   fc << "// Generated by kppcu: complex sparse LU of the mechanism (util/sutil.c:28-90),\n"

@@ -92,6 +92,9 @@ class Mechanism:
         L.kpp_b200_rosenbrock_host.argtypes = ros + [ctypes.c_int]
         L.kpp_b200_fun_jac.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 4
         L.kpp_b200_decomp_solve.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
+        L.kpp_b200_jac_vec.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int,
+                                       _vp]
+        L.kpp_b200_solve_tr.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
         L.kpp_b200_set_kernel.argtypes = [ctypes.c_int]
         L.kpp_b200_set_blocks_per_sm.argtypes = [ctypes.c_int]
         L.kpp_b200_sdirk.argtypes = ([ctypes.c_int, ctypes.c_int] + [_vp] * 9
@@ -421,6 +424,34 @@ class Mechanism:
         self._check(self.lib.kpp_b200_decomp_solve(ld, ld, _ptr(jvs), _ptr(x), _ptr(ising),
                                                    _vp(s.cuda_stream)))
         return ising
+
+    def jac_vec(self, jvs: torch.Tensor, uv: torch.Tensor, transposed: bool = False,
+                out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        """Batched J uv or J^T uv (kpp_b200_jac_vec; Jac_SP_Vec / JacTR_SP_Vec)
+        with jvs [LU_NONZERO, ld] and uv [NVAR, ld]."""
+        self._dev(jvs, torch.float64, "jvs")
+        self._dev(uv, torch.float64, "uv")
+        ld = jvs.shape[1]
+        if out is None:
+            out = torch.empty_like(uv)
+        s = stream if stream is not None else torch.cuda.current_stream(jvs.device)
+        self._check(self.lib.kpp_b200_jac_vec(ld, ld, _ptr(jvs), _ptr(uv), _ptr(out),
+                                              1 if transposed else 0, _vp(s.cuda_stream)))
+        return out
+
+    def solve_tr(self, jvs: torch.Tensor, x: torch.Tensor, out: Optional[torch.Tensor] = None,
+                 stream=None) -> torch.Tensor:
+        """Batched solve of (LU)^T xx = x for factorised jvs (kpp_b200_solve_tr;
+        KppSolveTR)."""
+        self._dev(jvs, torch.float64, "jvs")
+        self._dev(x, torch.float64, "x")
+        ld = jvs.shape[1]
+        if out is None:
+            out = torch.empty_like(x)
+        s = stream if stream is not None else torch.cuda.current_stream(jvs.device)
+        self._check(self.lib.kpp_b200_solve_tr(ld, ld, _ptr(jvs), _ptr(x), _ptr(out),
+                                               _vp(s.cuda_stream)))
+        return out
 
     # -- INTEGRATE-style driver -------------------------------------------
     def integrate(self, var, fix, temp, tin, tout, atol, rtol, method: str = "rodas3",

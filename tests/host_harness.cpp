@@ -22,6 +22,9 @@ using std::rint;
 // the device cosine of Update_SUN, for its own test
 extern "C" double host_cos_cr(double x) { return kpp_cos_cr(x); }
 #include KPP_MECH_HEADER
+#ifdef KPP_ADJ_HEADER
+#include KPP_ADJ_HEADER
+#endif
 
 extern "C" {
 
@@ -44,5 +47,17 @@ void host_jac(const double* var, const double* fix, const double* rconst, double
 int host_decomp(double* jvs) { return kpp_decomp(jvs); }
 
 void host_solve(const double* jvs, double* x) { kpp_solve(jvs, x); }
+
+#ifdef KPP_ADJ_HEADER
+void host_jac_sp_vec(const double* jvs, const double* uv, double* juv) {
+  kpp_jac_sp_vec(jvs, uv, juv);
+}
+
+void host_jactr_sp_vec(const double* jvs, const double* uv, double* jtuv) {
+  kpp_jactr_sp_vec(jvs, uv, jtuv);
+}
+
+void host_solve_tr(const double* jvs, const double* x, double* xx) { kpp_solve_tr(jvs, x, xx); }
+#endif
 
 }

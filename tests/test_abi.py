@@ -102,6 +102,12 @@ def test_entry_points_reject_bad_arguments_without_gpu():
     assert rc == 1 and b"null" in lib.kpp_b200_last_error()
     assert lib.kpp_b200_runge_kutta(0, 0, None, None, None, None, None, None, None, None, None,
                                     ip, rp, None, None, None, None) == 0
+    # the adjoint building blocks
+    assert lib.kpp_b200_jac_vec(4, 2, None, None, None, 0, None) == 1
+    assert lib.kpp_b200_jac_vec(4, 4, None, None, None, 0, None) == 1
+    assert b"null" in lib.kpp_b200_last_error()
+    assert lib.kpp_b200_solve_tr(4, 4, None, None, None, None) == 1
+    assert lib.kpp_b200_jac_vec(0, 0, None, None, None, 1, None) == 0
     # and the host-array entries of both
     for entry in (lib.kpp_b200_sdirk_host, lib.kpp_b200_runge_kutta_host):
         rc = entry(4, 2, None, None, None, None, None, None, None, None, None, ip, rp, None, None,

@@ -142,8 +142,10 @@ def _host_lib(mech, tmp_path):
     cxx = shutil.which("g++")
     out = tmp_path / f"host_{mech}.so"
     # -O without FMA contraction on x86-64: the reference's own flags
+    adj = REPO / "kpp_b200" / "_gen" / f"{mech}_adj.cuh"
+    extra = [f'-DKPP_ADJ_HEADER="{adj}"'] if adj.exists() else []
     subprocess.run([cxx, "-O", "-fPIC", "-shared", "-std=c++17", "-I", str(REPO / "kpp_b200" / "csrc"),
-                    f'-DKPP_MECH_HEADER="{hdr}"', str(REPO / "tests" / "host_harness.cpp"),
+                    f'-DKPP_MECH_HEADER="{hdr}"', *extra, str(REPO / "tests" / "host_harness.cpp"),
                     "-o", str(out)], check=True)
     lib = ctypes.CDLL(str(out))
     lib.host_rates.argtypes = [ctypes.c_double] * 4 + [ctypes.c_void_p] * 3
@@ -199,3 +201,44 @@ def test_rate_classes_are_reported(tmp_path):
     text = hdr.read_text()
     assert "#define KPP_RATES_DYNAMIC 0" in text
     assert "#define KPP_RATES_SUN 30" in text
+
+
+@pytest.mark.skipif(not ensure_built(), reason="oracle libraries not built")
+@pytest.mark.parametrize("mech", MECHS + ["mcm_isoprene"])
+def test_adjoint_building_blocks_bit_identical_on_host(mech, tmp_path, golden_dir):
+    """Jac_SP_Vec, JacTR_SP_Vec and KppSolveTR (src/gen.c:1763-1880,
+    2036-2120), as kppcu emits them (<mech>_adj.cuh) and compiled for the
+    host, against the reference's generated functions: bit for bit, on the
+    golden Jacobians and on their factorised Rosenbrock matrices."""
+    if not (REPO / "kpp_b200" / "_gen" / f"{mech}_adj.cuh").exists():
+        pytest.skip("generated adjoint header not present (run the build)")
+    h = _host_lib(mech, tmp_path)
+    for nm in ("host_jac_sp_vec", "host_jactr_sp_vec", "host_solve_tr"):
+        getattr(h, nm).argtypes = [ctypes.c_void_p] * 3
+    o = OracleLib(mech)
+    ref = o.lib
+    for nm in ("Jac_SP_Vec", "JacTR_SP_Vec", "KppSolveTR"):
+        getattr(ref, nm).argtypes = [ctypes.c_void_p] * 3
+    ref.KppDecomp.argtypes = [ctypes.c_void_p]
+    diag = o.lu_pattern()[3][: o.nvar]
+    g = np.load(golden_dir / f"funjac_{mech}.npz")
+    rng = np.random.default_rng(9)
+    for c in range(g["jvs"].shape[1]):
+        jvs = np.ascontiguousarray(g["jvs"][:, c])
+        uv = rng.standard_normal(o.nvar)
+        for host_fn, ref_fn in ((h.host_jac_sp_vec, ref.Jac_SP_Vec),
+                                (h.host_jactr_sp_vec, ref.JacTR_SP_Vec)):
+            a, b = np.zeros(o.nvar), np.zeros(o.nvar)
+            host_fn(_p(jvs), _p(uv), _p(a))
+            ref_fn(_p(jvs), _p(uv), _p(b))
+            np.testing.assert_array_equal(a, b)
+        # the factorised Rosenbrock matrix 1/(h gamma) - J, then the solve
+        e = -jvs.copy()
+        e[diag] += 1.0 / (10.0 * 0.5)
+        if ref.KppDecomp(_p(e)) != 0:
+            continue
+        x = rng.standard_normal(o.nvar)
+        a, b = np.zeros(o.nvar), np.zeros(o.nvar)
+        h.host_solve_tr(_p(e), _p(x), _p(a))
+        ref.KppSolveTR(_p(e), _p(x), _p(b))
+        np.testing.assert_array_equal(a, b)
