@@ -40,9 +40,10 @@ def test_jacobian_products_and_transposed_solve_bit_identical(mech, golden_dir):
     for transposed, ref_fn in ((False, ref.Jac_SP_Vec), (True, ref.JacTR_SP_Vec)):
         got = m.jac_vec(d(jvs), d(uv), transposed=transposed).cpu().numpy()
         for c in range(n):
+            # named arrays: the pointers handed to C must outlive the call
+            jc, uc = np.ascontiguousarray(jvs[:, c]), np.ascontiguousarray(uv[:, c])
             want = np.zeros(o.nvar)
-            ref_fn(_p(np.ascontiguousarray(jvs[:, c])), _p(np.ascontiguousarray(uv[:, c])),
-                   _p(want))
+            ref_fn(_p(jc), _p(uc), _p(want))
             np.testing.assert_array_equal(got[:, c], want)
     # factorised Rosenbrock matrices 1/(h gamma) - J, factorised by the reference
     e = -jvs.copy()
@@ -58,7 +59,7 @@ def test_jacobian_products_and_transposed_solve_bit_identical(mech, golden_dir):
     for c in range(n):
         if not ok[c]:
             continue
+        ec, xc = np.ascontiguousarray(e[:, c]), np.ascontiguousarray(x[:, c])
         want = np.zeros(o.nvar)
-        ref.KppSolveTR(_p(np.ascontiguousarray(e[:, c])), _p(np.ascontiguousarray(x[:, c])),
-                       _p(want))
+        ref.KppSolveTR(_p(ec), _p(xc), _p(want))
         np.testing.assert_array_equal(got[:, c], want)
