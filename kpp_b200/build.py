@@ -14,7 +14,7 @@ mechanism file and under $KPP_HOME/models (KPP's own layout).  Without them
 (for example on a machine that received prebuilt libraries) the existing
 libraries are kept; a missing library is an error.
 
-Usage: python -m kpp_b200.build [mech ...] [--all] [--force] [--jobs N]
+Usage: python -m kpp_b200.build [mech ...] [--all] [--force] [--jobs N] [--kpp-home DIR]
 """
 from __future__ import annotations
 
@@ -54,13 +54,9 @@ SCRATCH_LU_NONZERO = 200
 _LINE_MARKER = re.compile(rb"\s*#\s*(line\b|\d)")
 
 def default_kpp_home() -> str:
-    home = os.environ.get("KPP_HOME", "")
-    if home:
-        return home
-    for cand in ("/root/reference",):
-        if (Path(cand) / "models").is_dir():
-            return cand
-    return ""
+    """KPP's source tree (models/, examples/) from $KPP_HOME; empty when unset,
+    and the build then keeps the prebuilt libraries."""
+    return os.environ.get("KPP_HOME", "")
 
 
 def nvcc() -> str:
@@ -260,8 +256,9 @@ def default_mechanisms():
     return [m for m in all_mechanisms() if m not in ON_REQUEST or library_path(m).exists()]
 
 
-def build(mechs=None, force: bool = False, jobs: int | None = None, verbose: bool = True):
-    kpp_home = default_kpp_home()
+def build(mechs=None, force: bool = False, jobs: int | None = None, verbose: bool = True,
+          kpp_home: str | None = None):
+    kpp_home = kpp_home if kpp_home is not None else default_kpp_home()
     jobs = jobs or os.cpu_count() or 4
     mechs = mechs or default_mechanisms()
     built = {"util": build_util(force), "sched": build_sched(force)}
@@ -286,8 +283,11 @@ def main(argv=None):
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--all", action="store_true", help="also the on-request mechanisms")
+    ap.add_argument("--kpp-home", default=None,
+                    help="KPP source tree with models/ and examples/ (default: $KPP_HOME)")
     a = ap.parse_args(argv)
-    build(a.mechs or (all_mechanisms() if a.all else None), force=a.force, jobs=a.jobs)
+    build(a.mechs or (all_mechanisms() if a.all else None), force=a.force, jobs=a.jobs,
+          kpp_home=a.kpp_home)
 
 
 if __name__ == "__main__":

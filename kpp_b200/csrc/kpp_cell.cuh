@@ -168,6 +168,12 @@ struct LaunchArgs {
   double chain_dt;
 };
 
+// Whether the warp-per-cell kernel (kpp_coop.cuh) can integrate a launch: the
+// mechanism has its tables and every rate constant is fixed for the call.
+inline bool coop_supports(const LaunchArgs& a) {
+  return KPP_COOP && KPP_RATES_DYNAMIC == 0 && (KPP_RATES_SUN == 0 || a.sun != nullptr);
+}
+
 struct Stats {
   int nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng;
 };

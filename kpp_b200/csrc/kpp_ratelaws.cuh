@@ -57,10 +57,13 @@ __device__ __forceinline__ double kpp_fall(double TEMP, double CFACTOR, float A0
 // returns the correctly rounded value except when the exact result lies
 // within ~2^-100 of a rounding boundary.
 //   * argument reduction (Cody and Waite): x = k*pi/2 + r, |r| <= pi/4, with
-//     pi/2 split into three doubles so that r is exact to ~2^-150;
+//     pi/2 split into three doubles so that r is exact to ~2^-150; valid for
+//     |k| <= 3, i.e. |x| <= 4 (k*P1 is then exact); Update_SUN only passes
+//     |x| <= pi;
 //   * cos(r) and sin(r) by their Taylor series (16 terms each), evaluated by
-//     Horner's rule in double-double arithmetic (Dekker's exact sum and
-//     product; QD library formulation by Hida, Li and Bailey);
+//     Horner's rule in double-double arithmetic (Knuth's TwoSum and Dekker's
+//     FastTwoSum and exact product, here through an FMA; the double-double
+//     operations as formulated for the QD library by Hida, Li and Bailey);
 //   * cos(x) = cos(r), -sin(r), -cos(r), sin(r) for k = 0, 1, 2, 3 (mod 4).
 // Constants: pi/2 and (-1)^n/(2n)!, (-1)^n/(2n+1)! rounded to double-double.
 // ---------------------------------------------------------------------------

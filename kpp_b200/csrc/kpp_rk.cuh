@@ -500,7 +500,7 @@ __device__ __forceinline__ int decomp(const Method& m, double h, W& w, Stats& st
 #pragma unroll 4
   for (int i = 0; i < LU_NZ; i++) w.e1[i] = -w.fjac[i];
   kpp_add_diagonal(w.e1, gamma_h);
-  int ising = kpp_decomp(w.e1);
+  int ising = kpp_decomp(w.e1, w.wr);  // wr: the complex LU's work row, free here
   if (ising != 0) {
     st.ndec++;
     return ising;

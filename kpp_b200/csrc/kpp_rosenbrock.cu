@@ -79,7 +79,7 @@ __device__ __forceinline__ bool prepare_matrix(const CellEnv& env, double t, dou
     kpp_jac_sp<true>(w.y, env.fix, w.rconst, w.jvs, w.b);
     double ghinv = 1.0 / (direction * h * gam);
     kpp_add_diagonal(w.jvs, ghinv);
-    int ising = kpp_decomp(w.jvs);
+    int ising = kpp_decomp(w.jvs, w.yerr);  // Yerr is free here: the work row
     st.ndec++;
     if (ising == 0) return false;
     st.nsng++;
@@ -279,17 +279,31 @@ inline int check_launch(const char* what) {
 
 constexpr int kBlock = 128;
 
+// Set-up done once per device: `get` runs f(device) the first time it is
+// called with that device current (under a lock, so concurrent first calls
+// from several host threads do it once) and returns the value f gave.
+struct DeviceOnce {
+  std::mutex mu;
+  std::map<int, int> value;
+  template <class F>
+  int get(F f) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = value.find(dev);
+    if (it == value.end()) it = value.emplace(dev, f(dev)).first;
+    return it->second;
+  }
+};
+
 // Launcher and occupancy of the kernel of method M, defined in part M.
 template <int M>
 int launch_method(LaunchArgs& a, int grid, cudaStream_t s);
 template <int M>
 int occupancy_method();
-// The warp-cooperative kernel of method M (one warp per cell in shared
-// memory); `rates` holds the cells' fixed rate constants [NREACT][rates_ld].
+// The warp-per-cell kernel of method M (kpp_coop.cuh).
 template <int M>
-int launch_method_warp(LaunchArgs& a, const double* rates, long rates_ld, cudaStream_t s);
-// Shared memory per cell of the warp kernel (bytes).
-size_t warp_smem_bytes();
+int launch_method_coop(LaunchArgs& a, cudaStream_t s);
 // The SDIRK kernel (KPP_PART 6).
 int launch_sdirk(LaunchArgs& a, int grid, cudaStream_t s);
 
@@ -410,14 +424,15 @@ rosenbrock_kernel(const LaunchArgs a) {
 
 template <int M>
 int launch_method(LaunchArgs& a, int grid, cudaStream_t s) {
-  static bool l1_set = false;  // the kernel uses no shared memory: all of it as L1
-  if (!l1_set) {
+  // the kernel uses no shared memory: all of it as L1 (a per-device attribute)
+  static DeviceOnce carveout;
+  carveout.get([](int) {
     cudaFuncSetAttribute(rosenbrock_kernel<M, true>,
                          cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     cudaFuncSetAttribute(rosenbrock_kernel<M, false>,
                          cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    l1_set = true;
-  }
+    return 1;
+  });
   if (a.queue)
     rosenbrock_kernel<M, true><<<grid, kBlock, 0, s>>>(a);
   else
@@ -440,31 +455,42 @@ template int launch_method<KPP_PART>(LaunchArgs&, int, cudaStream_t);
 template int occupancy_method<KPP_PART>();
 #endif
 
-#include "kpp_warp.cuh"
+#if KPP_COOP
+#include "kpp_coop.cuh"
 
+// The warp-per-cell kernel of method M: one CTA of W warps per SM (shared
+// memory holds the tables and W cells), at most one CTA per W cells.
 template <int M>
-int launch_method_warp(LaunchArgs& a, const double* rates, long rates_ld, cudaStream_t s) {
-  static int grid_cap = 0;  // resident warps on this device (one per block)
-  if (grid_cap == 0) {
-    int dev = 0, sms = 1, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(warpk::kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)warpk::kSmemBytes);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warpk::kernel<M>, 32,
-                                                      warpk::kSmemBytes) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-    grid_cap = sms * per_sm;
-  }
-  const int grid = a.ncells < grid_cap ? a.ncells : grid_cap;
-  warpk::kernel<M><<<grid, 32, warpk::kSmemBytes, s>>>(a, rates, rates_ld);
-  return check_launch("warp rosenbrock kernel");
+int launch_method_coop(LaunchArgs& a, cudaStream_t s) {
+  constexpr int S = make_tableau(M).S;
+  constexpr int W = coop::warps_per_cta<S>();
+  constexpr size_t bytes = coop::smem_bytes<S>();
+  static_assert(W >= 1, "kppcu only writes tables for cells that fit shared memory");
+  static DeviceOnce sms_of;  // SMs of the device, with the kernels' attributes set there
+  const int sms = sms_of.get([](int dev) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    if (cudaFuncSetAttribute(coop::kernel<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes) != cudaSuccess ||
+        cudaFuncSetAttribute(coop::kernel<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes) != cudaSuccess)
+      return -1;
+    return n;
+  });
+  if (sms < 1) return fail(KPP_B200_ECUDA, "warp-per-cell kernel: device set-up failed");
+  const long want = ((long)a.ncells + W - 1) / W;
+  const int grid = (int)(want < sms ? want : sms);
+  if (a.queue)
+    coop::kernel<M, true><<<grid, 32 * W, bytes, s>>>(a);
+  else
+    coop::kernel<M, false><<<grid, 32 * W, bytes, s>>>(a);
+  return check_launch("warp-per-cell rosenbrock kernel");
 }
 
 #if KPP_PART <= 5
-template int launch_method_warp<KPP_PART>(LaunchArgs&, const double*, long, cudaStream_t);
+template int launch_method_coop<KPP_PART>(LaunchArgs&, cudaStream_t);
 #endif
+#endif  // KPP_COOP
 
 #if KPP_PART == 6
 #include "kpp_sdirk.cuh"
@@ -561,44 +587,21 @@ int launch_rk(LaunchArgs& a, int grid, cudaStream_t s);
 
 thread_local char g_last_error[512] = "";
 
-// Rate constants that are fixed for a whole call (those depending only on
-// TEMP/CFACTOR, and the SUN-dependent ones when SUN is given per cell), one
-// thread per cell, into rates [NREACT][rates_ld]: the input of the warp
-// kernel, which keeps them in shared memory.
-__global__ void __launch_bounds__(128) rates_kernel(const LaunchArgs a, double* rates,
-                                                    long rates_ld) {
-  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cell >= a.ncells) return;
-  CellEnv env;
-  load_env(env, a.temp, a.cfactor, a.sun, a.fix, a.ld, cell);
-  struct Col {
-    double* p;
-    long s;
-    __device__ __forceinline__ double& operator[](int i) const { return p[(long)i * s]; }
-  } r{rates + cell, rates_ld}, v{a.var + cell, a.ld};
-  kpp_rconst_static(r, a.tstart[cell], env.temp, env.cfactor, 0.0, v, env.fix);
-  if (env.sun_fixed >= 0.0)
-    kpp_rconst_sun(r, a.tstart[cell], env.temp, env.cfactor, env.sun_fixed, v, env.fix);
-}
-
-size_t warp_smem_bytes() {
-  return sizeof(double) * (size_t)(6 * NVAR + 6 * NVAR + LU_NZ + NREACT +
-                                   (NREACT > kpp_warp::NB ? NREACT : kpp_warp::NB) + NFIX + 1);
-}
-
-// Which kernel integrates: 0 automatic (warp-cooperative for mechanisms with
-// a scratch work set that fits shared memory, else thread per cell), 1 thread
-// per cell, 2 warp per cell.
+// Which kernel integrates: 0 automatic, 1 thread per cell, 2 warp per cell
+// (kpp_coop.cuh).  The warp-per-cell kernel runs only launches whose rate
+// constants are fixed for the call; the others always use the thread kernel.
 int g_kernel_choice = 0;
+// What the automatic choice picks for launches the warp-per-cell kernel supports.
+constexpr bool kCoopByDefault = false;
 
-bool use_warp_kernel() {
-#if defined(KPP_SCRATCH)
-  // Auto picks the thread-per-cell kernel: on saprc99 (fresh cells) it
-  // measured 1.45x faster than the warp kernel, whose time goes to the
-  // sequential pivot / solve phases.
-  if (g_kernel_choice != 2) return false;
-  return warp_smem_bytes() <= 200 * 1024;
+bool use_coop(const LaunchArgs& a) {
+#if KPP_COOP
+  if (!coop_supports(a)) return false;
+  if (g_kernel_choice == 2) return true;
+  if (g_kernel_choice == 1) return false;
+  return kCoopByDefault;
 #else
+  (void)a;
   return false;
 #endif
 }
@@ -655,7 +658,8 @@ __global__ void __launch_bounds__(128) decomp_solve_kernel(int ncells, int ld, d
   const int cell = blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= ncells) return;
   StridedLd jvs{jvs_g + cell, ld};
-  ising[cell] = kpp_decomp(jvs);
+  double wrow[NVAR];  // work row of the loop-form LU of large mechanisms
+  ising[cell] = kpp_decomp(jvs, wrow);
   if (x_g) {
     StridedLd x{x_g + cell, ld};
     kpp_solve(jvs, x);
@@ -785,43 +789,16 @@ int cached_counter(cudaStream_t stream, int** out) {
 
 size_t scratch_capacity_doubles(const LaunchArgs& a) { return a.scratch_doubles; }
 
-int launch_warp(LaunchArgs& a, cudaStream_t s) {
-  // The rate pre-pass writes into the work buffer (which the warp kernel does
-  // not otherwise need), in chunks of cells that fit it.
-  const long cap = (long)(scratch_capacity_doubles(a) / NREACT);
-  if (cap < 1) return fail(KPP_B200_EINVAL, "work buffer too small for the rate constants");
-  for (long c0 = 0; c0 < a.ncells; c0 += cap) {
-    LaunchArgs b = a;
-    const long n = (a.ncells - c0 < cap) ? a.ncells - c0 : cap;
-    b.ncells = (int)n;
-    b.var = a.var + c0;
-    b.fix = a.fix ? a.fix + c0 : nullptr;
-    b.temp = a.temp + c0;
-    b.cfactor = a.cfactor ? a.cfactor + c0 : nullptr;
-    b.sun = a.sun ? a.sun + c0 : nullptr;
-    b.tstart = a.tstart + c0;
-    b.tend = a.tend + c0;
-    b.hstart = a.hstart ? a.hstart + c0 : nullptr;
-    b.istatus = a.istatus + c0;
-    b.rstatus = a.rstatus + c0;
-    b.ierr = a.ierr + c0;
-    rates_kernel<<<(int)((n + kBlock - 1) / kBlock), kBlock, 0, s>>>(b, a.scratch, n);
-    int rc = check_launch("rates_kernel");
-    if (rc != KPP_B200_OK) return rc;
-    switch (b.ipar[3]) {
-      case 1: rc = launch_method_warp<1>(b, a.scratch, n, s); break;
-      case 2: rc = launch_method_warp<2>(b, a.scratch, n, s); break;
-      case 3: rc = launch_method_warp<3>(b, a.scratch, n, s); break;
-      case 5: rc = launch_method_warp<5>(b, a.scratch, n, s); break;
-      default: rc = launch_method_warp<4>(b, a.scratch, n, s); break;
-    }
-    if (rc != KPP_B200_OK) return rc;
-  }
-  return KPP_B200_OK;
-}
-
 int launch_rosenbrock(LaunchArgs& a, cudaStream_t s) {
-  if (use_warp_kernel() && a.scratch && !a.queue && a.nchain == 0) return launch_warp(a, s);
+  if (use_coop(a)) {
+    switch (a.ipar[3]) {
+      case 1: return launch_method_coop<1>(a, s);
+      case 2: return launch_method_coop<2>(a, s);
+      case 3: return launch_method_coop<3>(a, s);
+      case 5: return launch_method_coop<5>(a, s);
+      default: return launch_method_coop<4>(a, s);
+    }
+  }
   const int grid = (int)(a.nslots / kBlock);
   // Invalid methods are reported per cell by the validation in
   // rosenbrock_cell (IERR = -2); any valid instance does that.
@@ -889,8 +866,10 @@ static __device__ __align__(256) double g_static_scratch[(size_t)kScratchPerSlot
 
 // Device address of g_static_scratch on the current device (nullptr for
 // mechanisms whose work arrays are thread-local).  Looked up with
-// cudaGetSymbolAddress on the first call per device, with that device current.
-int static_scratch(double** out) {
+// cudaGetSymbolAddress on the first call per device, with that device current;
+// that first call is refused while `stream` is being captured (the lookup can
+// load the module, which a capture must not see).
+int static_scratch(cudaStream_t stream, double** out) {
   *out = nullptr;
 #if defined(KPP_SCRATCH)
   static std::mutex mu;
@@ -901,6 +880,13 @@ int static_scratch(double** out) {
   std::lock_guard<std::mutex> lock(mu);
   auto it = addr.find(dev);
   if (it == addr.end()) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(stream, &cap);
+    if (e != cudaSuccess) return cuda_fail("cudaStreamIsCapturing", e);
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(KPP_B200_EINVAL,
+                  "kpp_b200_rosenbrock_static: the first call on a device must come before any "
+                  "stream capture (call once before capture)");
     double* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, g_static_scratch);
     if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress(g_static_scratch)", e);
@@ -1022,9 +1008,11 @@ int host_pipeline(int ncells, int ld, double* var, const double* fix, const doub
     a.nslots = slots_for((int)n);
     int rc;
     if (which == 0) {
-      rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
-      if (rc != KPP_B200_OK) return rc;
-      a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+      if (!use_coop(a)) {  // the warp-per-cell kernel needs no work buffer
+        rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+        if (rc != KPP_B200_OK) return rc;
+        a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+      }
       rc = launch_rosenbrock(a, s);
     } else {
       const long per = which == 1 ? kSdirkPerSlot : kRkPerSlot;
@@ -1176,10 +1164,12 @@ int kpp_b200_rosenbrock(int ncells, int ld, double* var, const double* fix, cons
                      rpar, hstart, istatus, rstatus, ierr);
   if (rc != KPP_B200_OK || ncells == 0) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  a.nslots = slots_for(ncells);
-  rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
-  if (rc != KPP_B200_OK) return rc;
-  a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+  if (!use_coop(a)) {  // the warp-per-cell kernel needs no work buffer
+    a.nslots = slots_for(ncells);
+    rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+    if (rc != KPP_B200_OK) return rc;
+    a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+  }
   return launch_rosenbrock(a, s);
 }
 
@@ -1238,10 +1228,12 @@ int kpp_b200_rosenbrock_chain(int ncells, int ld, double* var, const double* fix
   a.nchain = ncalls;
   a.chain_dt = dt;
   a.order = order;
-  a.nslots = slots_for(ncells);
-  rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
-  if (rc != KPP_B200_OK) return rc;
-  a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+  if (!use_coop(a)) {  // the warp-per-cell kernel needs no work buffer
+    a.nslots = slots_for(ncells);
+    rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
+    if (rc != KPP_B200_OK) return rc;
+    a.scratch_doubles = scratch_bytes(a.nslots) / sizeof(double);
+  }
   rc = cached_counter(s, &a.queue);
   if (rc != KPP_B200_OK) return rc;
   cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(int), s);
@@ -1264,7 +1256,7 @@ int kpp_b200_rosenbrock_ws(int ncells, int ld, double* var, const double* fix, c
                      rpar, hstart, istatus, rstatus, ierr);
   if (rc != KPP_B200_OK || ncells == 0) return rc;
   a.nslots = slots_for(ncells);
-  if (kUsesScratch) {
+  if (kUsesScratch && !use_coop(a)) {
     if (!workspace || workspace_bytes < scratch_bytes(a.nslots))
       return fail(KPP_B200_EINVAL, "workspace smaller than kpp_b200_workspace_bytes()");
     a.scratch = (double*)workspace;
@@ -1291,7 +1283,7 @@ int kpp_b200_rosenbrock_static(int ncells, int ld, double* var, const double* fi
   }
   // one thread slot per cell, in whole blocks: at most kStaticMaxCells slots
   a.nslots = ((long)ncells + kBlock - 1) / kBlock * kBlock;
-  rc = static_scratch(&a.scratch);
+  rc = static_scratch((cudaStream_t)stream, &a.scratch);
   if (rc != KPP_B200_OK) return rc;
   a.scratch_doubles = a.scratch ? (size_t)kScratchPerSlot * kStaticMaxCells : 0;
   return launch_rosenbrock(a, (cudaStream_t)stream);
@@ -1390,7 +1382,13 @@ int kpp_b200_set_kernel(int which) {
   return KPP_B200_OK;
 }
 
-int kpp_b200_get_kernel(void) { return use_warp_kernel() ? 2 : 1; }
+int kpp_b200_get_kernel(void) {
+#if KPP_COOP
+  return g_kernel_choice == 2 || (g_kernel_choice == 0 && kCoopByDefault) ? 2 : 1;
+#else
+  return 1;
+#endif
+}
 
 int kpp_b200_set_blocks_per_sm(int blocks) {
   if (blocks < 0 || blocks > 64) return fail(KPP_B200_EINVAL, "blocks per SM must be 0..64");

@@ -208,7 +208,7 @@ __device__ __forceinline__ void prepare_matrix(const CellEnv& env, double h, dou
 #pragma unroll 4
     for (int i = 0; i < LU_NZ; i++) w.e[i] = -w.fjac[i];
     kpp_add_diagonal(w.e, hgi);
-    ising = kpp_decomp(w.e);
+    ising = kpp_decomp(w.e, w.tmp);  // tmp is free here: the work row
     st.ndec++;
     if (ising != 0) {
       st.nsng++;

@@ -14,7 +14,8 @@
 // and a second header, <prefix>_cmplx.cuh, with the complex LU the
 // Runge-Kutta methods factorise (KppDecompCmplxR / KppSolveCmplxR of
 // util/sutil.c:28-90: unrolled in the same operation order, or for patterns
-// of 2000 entries or more the generic loops over the LU tables).
+// of 2000 entries or more the generic loops over the LU tables, as are the
+// real LU and solve of such mechanisms).
 //
 // Arithmetic is the reference's, operation for operation: expression trees
 // are built with the same constant folding (multiplying by a constant 1
@@ -30,6 +31,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <fstream>
 #include <memory>
 #include <set>
@@ -332,21 +334,292 @@ void emit_dtable(std::ostream& o, const char* name, const std::vector<double>& v
   o << "};\n";
 }
 
-// Schedules and operand tables of the warp-cooperative kernel, in which one
-// warp integrates one cell held in shared memory.  Every value is computed by
-// exactly the operation sequence of the unrolled functions above; only
-// independent computations run in parallel:
-//   Fun   A[j] products in parallel, then each Vdot row summed by one lane
-//   Jac   B products in parallel, then each JVS entry summed by one lane
-//   LU    right-looking by pivot: each element still gets its updates in
-//         increasing pivot order, the order of util/sutil.c's row loop
-//   solve forward by pivot (each row's terms in increasing column order);
-//         backward by dependency level, each row summed by one lane
-// Operand index convention for products: 0..NVAR-1 = V, NVAR.. = FIX, and
-// KPP_WOPND_ONE = the constant 1.0 (padding: x*1.0 == x exactly).
-void emit_warp_tables(std::ostream& o, const Mechanism& m) {
+// ---------------------------------------------------------------------------
+// Tables of the warp-per-cell kernel (csrc/kpp_coop.cuh)
+// ---------------------------------------------------------------------------
+// One warp integrates one cell whose work set sits in shared memory; its 32
+// lanes share every phase through static schedules computed here.  Every value
+// is produced by exactly the operation sequence of the unrolled functions
+// above; only operations that do not depend on each other run side by side:
+//   products  the equation rates A (Fun) and the partial derivatives B (Jac):
+//             product t on lane t % 32 in round t / 32, as the weight (rate
+//             constant times stoichiometric factor, the reference's leading
+//             factors) times the reactant concentrations in order
+//   sums      each Vdot row / Jacobian entry summed by one lane in equation
+//             order; outputs spread over lanes, longest sums first
+//   LU        the operations of util/sutil.c's loop (row entry divided by the
+//             pivot; pivot row times the multiplier subtracted) as a dependency
+//             graph, list-scheduled by longest remaining path into iterations
+//             separated by warp barriers, each iteration of one kind
+//   solves    forward and backward substitution: a lane owns a row's
+//             left-to-right sum and runs its terms as soon as their operands
+//             are final (written by another lane in an earlier iteration)
+// All tables are 32-bit words in one array that each CTA stages in shared
+// memory.  A phase that iterates holds, per iteration, how many entries each
+// lane runs (4-bit counts, eight lanes per word) and, per lane, its entries in
+// order (layout [position][lane], so the lanes of a warp read consecutive
+// words).
+// LU patterns of this many entries or more get the loop forms of KppDecomp,
+// KppSolve and the complex LU instead of unrolled code.
+constexpr int kGenericLu = 2000;
+
+constexpr int kCoopLanes = 32;
+constexpr int kCoopLuCap = 2;     // LU units per lane per iteration
+constexpr int kCoopSolveCap = 4;  // solve terms per lane per iteration
+
+int bits_for(long n) {
+  int b = 1;
+  while ((1L << b) < n) b++;
+  return b;
+}
+
+struct CoopStream {
+  std::vector<std::vector<unsigned>> lane = std::vector<std::vector<unsigned>>(kCoopLanes);
+  std::vector<std::vector<int>> count;  // [iteration][lane]
+  size_t max_len() const {
+    size_t n = 0;
+    for (auto& l : lane) n = std::max(n, l.size());
+    return n;
+  }
+  // entries as [position][lane], padded with `pad`
+  std::vector<unsigned> interleaved(unsigned pad) const {
+    const size_t len = max_len();
+    std::vector<unsigned> out(len * kCoopLanes, pad);
+    for (int l = 0; l < kCoopLanes; l++)
+      for (size_t k = 0; k < lane[l].size(); k++) out[k * kCoopLanes + l] = lane[l][k];
+    return out;
+  }
+  // per-iteration counts, eight 4-bit lanes per word
+  std::vector<unsigned> counts() const {
+    std::vector<unsigned> out;
+    for (auto& c : count)
+      for (int w = 0; w < kCoopLanes / 8; w++) {
+        unsigned word = 0;
+        for (int j = 0; j < 8; j++) word |= (unsigned)c[w * 8 + j] << (4 * j);
+        out.push_back(word);
+      }
+    return out;
+  }
+};
+
+// LU: units in the order of util/sutil.c's loop; entry = div<<31 | t<<2B | m<<B | s
+// (div: J[t] = J[t] / J[s]; else J[t] = J[t] + (-J[m]) * J[s]).
+CoopStream coop_schedule_lu(const Mechanism& m, int B) {
+  const int n = m.nvar;
+  std::vector<std::vector<int>> pos(n, std::vector<int>(n, -1));
+  for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
+  struct Unit { int div, t, mm, s; };
+  std::vector<Unit> u;
+  std::vector<std::vector<int>> deps;
+  std::vector<int> last(m.lu_nonzero, -1);
+  auto dep = [&](std::vector<int>& d, int e) {
+    if (last[e] >= 0) d.push_back(last[e]);
+  };
+  for (int k = 0; k < n; k++)
+    for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+      const int j = m.lu_icol[kk];
+      std::vector<int> d;
+      dep(d, kk);
+      dep(d, m.lu_diag[j]);
+      u.push_back({1, kk, 0, m.lu_diag[j]});
+      deps.push_back(d);
+      last[kk] = (int)u.size() - 1;
+      for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
+        const int t = pos[k][m.lu_icol[jj]];
+        std::vector<int> d2;
+        dep(d2, t);
+        dep(d2, kk);
+        dep(d2, jj);
+        u.push_back({0, t, kk, jj});
+        deps.push_back(d2);
+        last[t] = (int)u.size() - 1;
+      }
+    }
+  const int N = (int)u.size();
+  std::vector<std::vector<int>> succ(N);
+  std::vector<int> pending(N, 0), prio(N, 1);
+  for (int i = 0; i < N; i++) {
+    std::sort(deps[i].begin(), deps[i].end());
+    deps[i].erase(std::unique(deps[i].begin(), deps[i].end()), deps[i].end());
+    pending[i] = (int)deps[i].size();
+    for (int p : deps[i]) succ[p].push_back(i);
+  }
+  for (int i = N - 1; i >= 0; i--)
+    for (int s : succ[i]) prio[i] = std::max(prio[i], prio[s] + 1);
+  std::vector<int> ready;
+  for (int i = 0; i < N; i++)
+    if (pending[i] == 0) ready.push_back(i);
+  CoopStream st;
+  int left = N;
+  while (left > 0) {
+    std::sort(ready.begin(), ready.end(), [&](int a, int b) {
+      return prio[a] != prio[b] ? prio[a] > prio[b] : a < b;
+    });
+    const int kind = u[ready[0]].div;
+    std::vector<int> take, keep;
+    for (int r : ready)
+      if (u[r].div == kind && (int)take.size() < kCoopLuCap * kCoopLanes) take.push_back(r);
+      else keep.push_back(r);
+    std::vector<int> cnt(kCoopLanes, 0);
+    std::vector<int> next;
+    // the shortest lane streams take the first units of the iteration
+    std::vector<int> order(kCoopLanes);
+    for (int l = 0; l < kCoopLanes; l++) order[l] = l;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return st.lane[a].size() < st.lane[b].size(); });
+    for (size_t i = 0; i < take.size(); i++) {
+      const int l = order[i % kCoopLanes];
+      const Unit& x = u[take[i]];
+      st.lane[l].push_back((unsigned)x.div << 31 | (unsigned)x.t << (2 * B) |
+                           (unsigned)x.mm << B | (unsigned)x.s);
+      cnt[l]++;
+      left--;
+      for (int s : succ[take[i]])
+        if (--pending[s] == 0) next.push_back(s);
+    }
+    st.count.push_back(cnt);
+    ready = keep;
+    ready.insert(ready.end(), next.begin(), next.end());
+  }
+  return st;
+}
+
+// Forward (L, unit diagonal) or backward (U) substitution.  Entry =
+// a | c<<B | r<<(B+C) | start<<(B+2C) | end<<(B+2C+1) | noterm<<(B+2C+2):
+// start: acc = X[r]; a term: acc = acc - J[a]*X[c]; end: X[r] = acc, divided
+// by J[diag r] in the backward phase; noterm: a backward row without terms.
+CoopStream coop_schedule_solve(const Mechanism& m, bool backward, int B, int C) {
+  const int n = m.nvar;
+  std::vector<std::vector<std::pair<int, int>>> terms(n);
+  for (int r = 0; r < n; r++) {
+    const int b = backward ? m.lu_diag[r] + 1 : m.lu_crow[r];
+    const int e = backward ? m.lu_crow[r + 1] : m.lu_diag[r];
+    for (int j = b; j < e; j++) terms[r].push_back({j, m.lu_icol[j]});
+  }
+  const int INF = 1 << 30;
+  std::vector<int> fin(n, INF);
+  std::vector<char> started(n, 0);
+  int todo = 0;
+  for (int r = 0; r < n; r++) {
+    if (!backward && terms[r].empty()) {
+      fin[r] = -1;  // forward: unchanged, final from the start
+      started[r] = 1;
+    } else {
+      todo++;
+    }
+  }
+  // priority: terms still to run on the longest dependency path from the row
+  std::vector<std::vector<int>> users(n);
+  for (int r = 0; r < n; r++)
+    for (auto& t : terms[r]) users[t.second].push_back(r);
+  std::vector<int> tail(n, 0);
+  for (int step = 0; step < n; step++) {
+    const int r = backward ? step : n - 1 - step;  // users come after r in the phase
+    int best = 0;
+    for (int w : users[r]) best = std::max(best, tail[w]);
+    tail[r] = (int)terms[r].size() + 1 + best;
+  }
+  std::vector<int> row(kCoopLanes, -1), next_term(kCoopLanes, 0);
+  CoopStream st;
+  const unsigned S0 = 1u << (B + 2 * C), E0 = 1u << (B + 2 * C + 1), N0 = 1u << (B + 2 * C + 2);
+  for (int it = 0; todo > 0; it++) {
+    if (it > 100000) break;  // no progress: cannot happen for a triangular system
+    std::vector<int> cnt(kCoopLanes, 0);
+    // lanes with the shortest streams pick new rows first
+    std::vector<int> order(kCoopLanes);
+    for (int l = 0; l < kCoopLanes; l++) order[l] = l;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      return (row[a] >= 0) != (row[b] >= 0) ? row[a] >= 0 : st.lane[a].size() < st.lane[b].size();
+    });
+    for (int l : order) {
+      while (cnt[l] < kCoopSolveCap) {
+        if (row[l] < 0) {
+          int best = -1;
+          for (int r = 0; r < n; r++) {
+            if (started[r]) continue;
+            const bool ok = terms[r].empty() || fin[terms[r][0].second] < it;
+            if (ok && (best < 0 || tail[r] > tail[best])) best = r;
+          }
+          if (best < 0) break;
+          started[best] = 1;
+          row[l] = best;
+          next_term[l] = 0;
+        }
+        const int r = row[l];
+        if (terms[r].empty()) {  // backward row without terms: X[r] = X[r] / J[diag]
+          st.lane[l].push_back((unsigned)r << (B + C) | S0 | E0 | N0);
+          cnt[l]++;
+          fin[r] = it;
+          todo--;
+          row[l] = -1;
+          continue;
+        }
+        const int k = next_term[l];
+        const auto& t = terms[r][k];
+        if (fin[t.second] >= it) break;  // operand not final yet
+        const bool last = k + 1 == (int)terms[r].size();
+        st.lane[l].push_back((unsigned)t.first | (unsigned)t.second << B |
+                             (unsigned)r << (B + C) | (k == 0 ? S0 : 0u) | (last ? E0 : 0u));
+        cnt[l]++;
+        next_term[l]++;
+        if (last) {
+          fin[r] = it;
+          todo--;
+          row[l] = -1;
+        }
+      }
+    }
+    st.count.push_back(cnt);
+  }
+  return st;
+}
+
+// Sums: each output (a Vdot row or a Jacobian entry) is a left-to-right sum of
+// coefficient * product; outputs go to the least loaded lane, longest first.
+struct CoopSumLayout {
+  int src_bits, coef_bits, dst_bits;
+};
+std::vector<unsigned> coop_schedule_sums(const std::vector<std::vector<std::pair<int, int>>>& outs,
+                                         const std::vector<char>& diag, CoopSumLayout L,
+                                         int& per_lane) {
+  std::vector<int> idx(outs.size());
+  for (size_t i = 0; i < idx.size(); i++) idx[i] = (int)i;
+  auto cost = [&](int o) { return std::max<int>(1, (int)outs[o].size()); };
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  std::vector<std::vector<int>> lanes(kCoopLanes);
+  std::vector<int> load(kCoopLanes, 0);
+  for (int o : idx) {
+    int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lanes[l].push_back(o);
+    load[l] += cost(o);
+  }
+  CoopStream st;
+  const int F = L.src_bits + L.coef_bits;
+  for (int l = 0; l < kCoopLanes; l++)
+    for (int o : lanes[l]) {
+      const unsigned dst = (unsigned)o << (F + 4);
+      const unsigned dg = diag[o] ? 1u << (F + 3) : 0u;
+      if (outs[o].empty()) {
+        st.lane[l].push_back(dst | dg | 1u << (F + 2) | 1u << (F + 1) | 1u << F);
+        continue;
+      }
+      for (size_t k = 0; k < outs[o].size(); k++)
+        st.lane[l].push_back(dst | dg | (k + 1 == outs[o].size() ? 1u << (F + 1) : 0u) |
+                             (k == 0 ? 1u << F : 0u) |
+                             (unsigned)outs[o][k].second << L.src_bits |
+                             (unsigned)outs[o][k].first);
+    }
+  per_lane = (int)st.max_len();
+  return st.interleaved(0xFFFFFFFFu);
+}
+
+// The tables of csrc/kpp_coop.cuh for mechanism m (KPP_COOP 0 when the
+// mechanism exceeds the 32-bit packing: more than 1024 LU entries, 128
+// variable species, 255 extended-state entries or four reactant factors).
+void emit_coop_tables(std::ostream& o, const Mechanism& m) {
   View vw(m);
   const int nvar = m.nvar, nr = m.nreact();
+  const int next = m.nvar + m.nfix + 1;  // V, FIX, 1.0
   const int ONE = m.nvar + m.nfix;
   auto factors = [&](int eq, int skip, std::vector<int>& out) {
     for (int i = 0; i < nvar; i++) {
@@ -356,156 +629,154 @@ void emit_warp_tables(std::ostream& o, const Mechanism& m) {
     for (int i = nvar; i < m.nspec; i++)
       for (int c = 0; c < (int)vw.left(i, eq); c++) out.push_back(i);
   };
+  // constants: 1.0 first, then the sums' coefficients, then weight constants
+  std::vector<double> kc{1.0};
+  auto code = [&](double v) {
+    for (size_t i = 0; i < kc.size(); i++)
+      if (std::memcmp(&kc[i], &v, sizeof v) == 0) return (int)i;
+    kc.push_back(v);
+    return (int)kc.size() - 1;
+  };
+  // products of Fun (A, one per equation that changes a variable species) and
+  // of Jac_SP (B, one per reactant occurrence), with their weights
+  struct Prod { int rct; double k1, k2; std::vector<int> f; };
+  std::vector<Prod> pa, pb;
+  std::vector<int> a_of_eq(nr, -1);
   int maxf = 1;
-  // --- Fun products
-  std::vector<int> a_eq, a_rct, a_f;
-  std::vector<double> a_k1, a_k2;
-  std::vector<std::vector<int>> a_fs;
   for (int j = 0; j < nr; j++) {
     bool used = false;
     for (int i = 0; i < nvar; i++)
       if (vw.net(i, j) != 0) { used = true; break; }
     if (!used) continue;
     Head h = head_of(m, j, 1.0f);
-    std::vector<int> f;
-    factors(j, -1, f);
-    maxf = std::max(maxf, (int)f.size());
-    a_eq.push_back(j); a_rct.push_back(h.rct); a_k1.push_back(h.k1); a_k2.push_back(h.k2);
-    a_fs.push_back(f);
+    Prod p{h.rct, h.k1, h.k2, {}};
+    factors(j, -1, p.f);
+    maxf = std::max(maxf, (int)p.f.size());
+    a_of_eq[j] = (int)pa.size();
+    pa.push_back(p);
   }
-  // --- Jac products
-  std::vector<int> b_rct;
-  std::vector<double> b_k1, b_k2;
-  std::vector<std::vector<int>> b_fs;
   std::vector<std::vector<int>> bidx(nr, std::vector<int>(nvar, -1));
   for (int i = 0; i < nr; i++)
     for (int j = 0; j < nvar; j++) {
       if (vw.left(j, i) == 0) continue;
-      bidx[i][j] = (int)b_rct.size();
+      bidx[i][j] = (int)pb.size();
       Head h = head_of(m, i, vw.left(j, i));
-      std::vector<int> f;
-      factors(i, j, f);
-      maxf = std::max(maxf, (int)f.size());
-      b_rct.push_back(h.rct); b_k1.push_back(h.k1); b_k2.push_back(h.k2); b_fs.push_back(f);
+      Prod p{h.rct, h.k1, h.k2, {}};
+      factors(i, j, p.f);
+      maxf = std::max(maxf, (int)p.f.size());
+      pb.push_back(p);
     }
-  auto flat = [&](const std::vector<std::vector<int>>& fs) {
-    std::vector<int> out;
-    for (auto& f : fs)
-      for (int k = 0; k < maxf; k++) out.push_back(k < (int)f.size() ? f[k] : ONE);
-    return out;
-  };
-  // --- Vdot rows (CSR over species; terms in reaction order)
-  std::vector<int> v_ptr{0}, v_j;
-  std::vector<double> v_c;
-  for (int i = 0; i < nvar; i++) {
+  // sums: Vdot rows over A, Jacobian entries (LU pattern) over B
+  std::vector<std::vector<std::pair<int, int>>> vsum(nvar), jsum;
+  std::vector<char> vdiag(nvar, 0), jdiag;
+  for (int i = 0; i < nvar; i++)
     for (int j = 0; j < nr; j++) {
-      float c = vw.net(i, j);
-      if (c == 0) continue;
-      v_j.push_back(j);
-      v_c.push_back(const_value(c));
+      const float c = vw.net(i, j);
+      if (c != 0) vsum[i].push_back({a_of_eq[j], code(const_value(c))});
     }
-    v_ptr.push_back((int)v_j.size());
-  }
-  // --- JVS entries (CSR over LU positions; terms in reaction order)
-  std::vector<int> j_ptr{0}, j_b;
-  std::vector<double> j_c;
   for (int i = 0; i < nvar; i++)
     for (int j = 0; j < nvar; j++) {
       if (!(m.lustruct[i][j] || i == j)) continue;
+      std::vector<std::pair<int, int>> t;
       if (m.lustruct[i][j])
         for (int k = 0; k < nr; k++)
-          if (vw.net(i, k) * (bidx[k][j] >= 0 ? 1.0f : 0.0f) != 0) {
-            j_b.push_back(bidx[k][j]);
-            j_c.push_back(const_value(vw.net(i, k)));
-          }
-      j_ptr.push_back((int)j_b.size());
+          if (vw.net(i, k) * (bidx[k][j] >= 0 ? 1.0f : 0.0f) != 0)
+            t.push_back({bidx[k][j], code(const_value(vw.net(i, k)))});
+      jsum.push_back(t);
+      jdiag.push_back(i == j);
     }
-  // --- LU by pivot
-  std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
-  for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
-  std::vector<int> lu_piv, lu_lptr{0}, lu_l, lu_uptr{0}, lu_ut, lu_um, lu_us;
-  for (int j = 0; j < nvar; j++) {
-    std::vector<int> rows;
-    for (int k = j + 1; k < nvar; k++)
-      if (pos[k][j] >= 0) rows.push_back(k);
-    if (rows.empty()) continue;
-    lu_piv.push_back(j);
-    for (int k : rows) lu_l.push_back(pos[k][j]);
-    lu_lptr.push_back((int)lu_l.size());
-    for (int k : rows)
-      for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
-        lu_ut.push_back(pos[k][m.lu_icol[jj]]);
-        lu_um.push_back(pos[k][j]);
-        lu_us.push_back(jj);
+  const int ncoef = (int)kc.size();
+  std::vector<unsigned> wa, wb;  // weight words: rct | k1 code | k2 code
+  const int RB = bits_for(nr + 1);
+  auto weights = [&](const std::vector<Prod>& ps, std::vector<unsigned>& out) {
+    for (const Prod& p : ps)
+      out.push_back((unsigned)(p.rct >= 0 ? p.rct : nr) | (unsigned)code(p.k1) << RB |
+                    (unsigned)code(p.k2) << (RB + 12));
+  };
+  weights(pa, wa);
+  weights(pb, wb);
+  const int B = bits_for(m.lu_nonzero), C = bits_for(nvar);
+  CoopSumLayout SL{bits_for(std::max<size_t>({pa.size(), pb.size(), 2})), bits_for(ncoef),
+                   bits_for(std::max(m.lu_nonzero, nvar))};
+  const bool fits = m.lu_nonzero <= 1024 && nvar <= 128 && next <= 255 && maxf <= 4 &&
+                    (long)kc.size() <= 4096 && RB + 24 <= 32 &&
+                    SL.src_bits + SL.coef_bits + 4 + SL.dst_bits <= 32 &&
+                    B + 2 * C + 3 <= 32;
+  o << "\n// ---- tables of the warp-per-cell kernel (csrc/kpp_coop.cuh) ----\n";
+  if (!fits) {
+    o << "#define KPP_COOP 0\n";
+    return;
+  }
+  o << "#define KPP_COOP 1\nnamespace kpp_coop {\n";
+  auto prod_words = [&](const std::vector<Prod>& ps) {
+    const size_t rounds = (ps.size() + kCoopLanes - 1) / kCoopLanes;
+    std::vector<unsigned> out(rounds * kCoopLanes, 0);
+    for (size_t t = 0; t < out.size(); t++) {
+      unsigned w = 0;
+      for (int f = 0; f < 4; f++) {
+        const int idx = (t < ps.size() && f < (int)ps[t].f.size()) ? ps[t].f[f] : ONE;
+        w |= (unsigned)idx << (8 * f);
       }
-    lu_uptr.push_back((int)lu_ut.size());
+      out[t] = w;
+    }
+    return out;
+  };
+  std::vector<unsigned> fa = prod_words(pa), fb = prod_words(pb);
+  wa.resize(fa.size(), (unsigned)nr);
+  wb.resize(fb.size(), (unsigned)nr);
+  int lv = 0, lj = 0;
+  std::vector<unsigned> sv = coop_schedule_sums(vsum, vdiag, SL, lv);
+  std::vector<unsigned> sj = coop_schedule_sums(jsum, jdiag, SL, lj);
+  CoopStream lu = coop_schedule_lu(m, B);
+  CoopStream fw = coop_schedule_solve(m, false, B, C);
+  CoopStream bw = coop_schedule_solve(m, true, B, C);
+  std::vector<unsigned> diag(m.lu_diag.begin(), m.lu_diag.begin() + nvar);
+  struct Part { const char* name; std::vector<unsigned> words; };
+  std::vector<Part> parts = {
+      {"PF", fa}, {"WF", wa}, {"PJ", fb}, {"WJ", wb}, {"SV", sv}, {"SJ", sj},
+      {"CLU", lu.counts()}, {"LU", lu.interleaved(0)}, {"CFW", fw.counts()},
+      {"FW", fw.interleaved(0)}, {"CBW", bw.counts()}, {"BW", bw.interleaved(0)},
+      {"DIAG", diag}};
+  long total_words = 0;
+  for (auto& p : parts) total_words += (long)p.words.size();
+  // one cell of the six-stage method beside the tables must fit the 227 KB of
+  // shared memory a CTA can hold, and the rate constants are staged in the
+  // cell's matrix and product area
+  const long cell6 = 2L * next + 9L * nvar + m.lu_nonzero + (long)pa.size() +
+                     ((long)pb.size() > 7L * nvar ? (long)pb.size() : 0L);
+  const long table_bytes = (total_words * 4 + 15) / 16 * 16 + 8L * ncoef;
+  if (table_bytes + 8 * cell6 > 227L * 1024 || m.lu_nonzero + (long)pa.size() < nr) {
+    o << "}  // namespace kpp_coop\n#undef KPP_COOP\n#define KPP_COOP 0\n";
+    return;
   }
-  // --- forward solve by pivot
-  std::vector<int> fw_piv, fw_ptr{0}, fw_row, fw_pos;
-  for (int j = 0; j < nvar; j++) {
-    std::vector<int> rows;
-    for (int i = j + 1; i < nvar; i++)
-      if (pos[i][j] >= 0) rows.push_back(i);
-    if (rows.empty()) continue;
-    fw_piv.push_back(j);
-    for (int i : rows) { fw_row.push_back(i); fw_pos.push_back(pos[i][j]); }
-    fw_ptr.push_back((int)fw_row.size());
+  long off = 0;
+  std::vector<unsigned> all;
+  for (auto& p : parts) {
+    o << "constexpr int O_" << p.name << " = " << off << ";\n";
+    off += (long)p.words.size();
+    all.insert(all.end(), p.words.begin(), p.words.end());
   }
-  // --- backward solve by level: level(i) = 1 + max level(c), c > i in row i
-  std::vector<int> level(nvar, 0);
-  int nlev = 0;
-  for (int i = nvar - 1; i >= 0; i--) {
-    int lv = 0;
-    for (int jj = m.lu_diag[i] + 1; jj < m.lu_crow[i + 1]; jj++)
-      lv = std::max(lv, level[m.lu_icol[jj]] + 1);
-    level[i] = lv;
-    nlev = std::max(nlev, lv + 1);
-  }
-  std::vector<int> bw_lptr{0}, bw_rows;
-  for (int lv = 0; lv < nlev; lv++) {
-    for (int i = nvar - 1; i >= 0; i--)
-      if (level[i] == lv) bw_rows.push_back(i);
-    bw_lptr.push_back((int)bw_rows.size());
-  }
-
-  o << "\n// ---- schedules of the warp-cooperative kernel (one warp per cell) ----\n";
-  o << "namespace kpp_warp {\n";
-  o << "constexpr int KPP_WOPND_ONE = " << ONE << ";\n";
-  o << "constexpr int MAXF = " << maxf << ";\n";
-  o << "constexpr int NA = " << a_eq.size() << ", NB = " << b_rct.size()
-    << ", NPIV = " << lu_piv.size() << ", NFWP = " << fw_piv.size() << ", NLEV = " << nlev << ";\n";
-  emit_table(o, "int", "a_eq", a_eq);
-  emit_table(o, "int", "a_rct", a_rct);
-  emit_dtable(o, "a_k1", a_k1);
-  emit_dtable(o, "a_k2", a_k2);
-  emit_table(o, "short", "a_f", flat(a_fs));
-  emit_table(o, "int", "b_rct", b_rct);
-  emit_dtable(o, "b_k1", b_k1);
-  emit_dtable(o, "b_k2", b_k2);
-  emit_table(o, "short", "b_f", flat(b_fs));
-  emit_table(o, "int", "v_ptr", v_ptr);
-  emit_table(o, "short", "v_j", v_j);
-  emit_dtable(o, "v_c", v_c);
-  emit_table(o, "int", "j_ptr", j_ptr);
-  emit_table(o, "short", "j_b", j_b);
-  emit_dtable(o, "j_c", j_c);
-  emit_table(o, "int", "lu_diag", std::vector<int>(m.lu_diag.begin(), m.lu_diag.end() - 1));
-  emit_table(o, "int", "lu_piv", lu_piv);
-  emit_table(o, "int", "lu_lptr", lu_lptr);
-  emit_table(o, "short", "lu_l", lu_l);
-  emit_table(o, "int", "lu_uptr", lu_uptr);
-  emit_table(o, "short", "lu_ut", lu_ut);
-  emit_table(o, "short", "lu_um", lu_um);
-  emit_table(o, "short", "lu_us", lu_us);
-  emit_table(o, "int", "fw_piv", fw_piv);
-  emit_table(o, "int", "fw_ptr", fw_ptr);
-  emit_table(o, "short", "fw_row", fw_row);
-  emit_table(o, "short", "fw_pos", fw_pos);
-  emit_table(o, "int", "bw_lptr", bw_lptr);
-  emit_table(o, "short", "bw_rows", bw_rows);
-  emit_table(o, "int", "lu_crow", m.lu_crow);
-  emit_table(o, "short", "lu_icol", m.lu_icol);
-  o << "}  // namespace kpp_warp\n";
+  long sum_terms_v = 0, sum_terms_j = 0;
+  for (auto& s : vsum) sum_terms_v += (long)s.size();
+  for (auto& s : jsum) sum_terms_j += (long)s.size();
+  o << "constexpr int TAB_WORDS = " << off << ";\n"
+    << "constexpr int NEXT = " << next << ", ONE = " << ONE << ";\n"
+    << "constexpr int NA = " << pa.size() << ", NB = " << pb.size() << ", MAXF = " << maxf
+    << ";\n"
+    << "constexpr int RF = " << fa.size() / kCoopLanes << ", RJ = " << fb.size() / kCoopLanes
+    << ";  // product rounds\n"
+    << "constexpr int NKC = " << ncoef << ";\n"
+    << "constexpr int RATE_BITS = " << RB << ", NO_RATE = " << nr << ";\n"
+    << "constexpr int SUM_SRC_BITS = " << SL.src_bits << ", SUM_COEF_BITS = " << SL.coef_bits
+    << ";\n"
+    << "constexpr int LV = " << lv << ", LJ = " << lj << ";  // entries per lane of the sums ("
+    << sum_terms_v << " and " << sum_terms_j << " terms)\n"
+    << "constexpr int IT_LU = " << lu.count.size() << ", IT_FW = " << fw.count.size()
+    << ", IT_BW = " << bw.count.size() << ";  // iterations\n"
+    << "constexpr int LU_BITS = " << B << ", X_BITS = " << C << ";\n";
+  emit_table(o, "unsigned int", "tab", all);
+  emit_dtable(o, "kc", kc);
+  o << "}  // namespace kpp_coop\n";
 }
 
 }  // namespace
@@ -596,7 +867,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
        "// each inlined copy of a body of tens of thousands of operations, and one\n"
        "// call is negligible next to such a body.\n"
        "#ifndef KPP_MECH_INLINE\n"
-    << "#define KPP_MECH_INLINE " << (m.lu_nonzero >= 2000 ? "__noinline__" : "__forceinline__")
+    << "#define KPP_MECH_INLINE " << (m.lu_nonzero >= kGenericLu ? "__noinline__" : "__forceinline__")
     << "\n#endif\n\n";
   o << "// Species indices (variable species first, then fixed species).\n";
   for (int i = 0; i < nspec; i++) o << "#define ind_" << vw.name(i) << " " << i << "\n";
@@ -779,98 +1050,126 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     o << "  JVS[" << m.lu_diag[i] << "] = JVS[" << m.lu_diag[i] << "] + v;\n";
   o << "}\n\n";
 
-  // ---- KppDecomp, unrolled
-  {
+  // ---- KppDecomp and KppSolve.  Mechanisms below kGenericLu LU entries get
+  // both fully unrolled; larger ones (MCM isoprene: 7123 entries, a 41k
+  // operation LU) get the reference's own loops over the LU tables (in
+  // constant memory, read uniformly by a warp), the same operations in the
+  // same order: an unrolled body of tens of thousands of operations takes the
+  // device compiler many minutes per translation unit and runs from the
+  // instruction cache poorly.
+  const bool generic_lu = m.lu_nonzero >= kGenericLu;
+  if (generic_lu) {
+    auto table = [&](const char* name, const std::vector<int>& v) {
+      o << "__constant__ int " << name << "[" << v.size() << "] = {";
+      for (size_t i = 0; i < v.size(); i++) o << (i % 16 == 0 ? "\n    " : " ") << v[i] << ",";
+      o << "};\n";
+    };
+    o << "#define KPP_LU_GENERIC 1\n";
+    table("kpp_lu_crow_c", m.lu_crow);
+    table("kpp_lu_diag_c", m.lu_diag);
+    table("kpp_lu_icol_c", m.lu_icol);
+    for (int k = 0; k < nvar; k++)
+      for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+        const int j = m.lu_icol[kk];
+        ops_decomp += 1 + 2L * (m.lu_crow[j + 1] - m.lu_diag[j] - 1);
+      }
+    for (int i = 0; i < nvar; i++)
+      ops_solve += 2L * (m.lu_crow[i + 1] - m.lu_crow[i] - 1) + 1;
+    o << "\n"
+         "// In-place no-pivot sparse LU of one cell (KppDecomp, util/sutil.c:2-23), row by\n"
+         "// row through the dense work row W of NVAR entries; returns k+1 when the\n"
+         "// diagonal entry of row k is zero on entry to its elimination, 0 on success.\n"
+         "template <class TJ, class TW>\n"
+         "__device__ __noinline__ int kpp_decomp(TJ& JVS, TW& W) {\n"
+         "  for (int k = 0; k < KPP_NVAR; k++) {\n"
+         "    const int dk = kpp_lu_diag_c[k], b = kpp_lu_crow_c[k], e = kpp_lu_crow_c[k + 1];\n"
+         "    if (JVS[dk] == 0.0) return k + 1;\n"
+         "    for (int kk = b; kk < e; kk++) W[kpp_lu_icol_c[kk]] = JVS[kk];\n"
+         "    for (int kk = b; kk < dk; kk++) {\n"
+         "      const int j = kpp_lu_icol_c[kk];\n"
+         "      const double a = -W[j] / JVS[kpp_lu_diag_c[j]];\n"
+         "      W[j] = -a;\n"
+         "      for (int jj = kpp_lu_diag_c[j] + 1; jj < kpp_lu_crow_c[j + 1]; jj++) {\n"
+         "        const int c = kpp_lu_icol_c[jj];\n"
+         "        W[c] = W[c] + a*JVS[jj];\n"
+         "      }\n"
+         "    }\n"
+         "    for (int kk = b; kk < e; kk++) JVS[kk] = W[kpp_lu_icol_c[kk]];\n"
+         "  }\n"
+         "  return 0;\n"
+         "}\n\n"
+         "// Solve (LU) x = b in place, b given in X (KppSolve, src/gen.c:1960-2034: each\n"
+         "// row's terms subtracted left to right, the backward rows divided last).\n"
+         "template <class TJ, class TX>\n"
+         "__device__ __noinline__ void kpp_solve(const TJ& JVS, TX& X) {\n"
+         "  for (int i = 0; i < KPP_NVAR; i++) {\n"
+         "    const int b = kpp_lu_crow_c[i], d = kpp_lu_diag_c[i];\n"
+         "    if (b < d) {\n"
+         "      double x = X[i];\n"
+         "      for (int j = b; j < d; j++) x = x - JVS[j]*X[kpp_lu_icol_c[j]];\n"
+         "      X[i] = x;\n"
+         "    }\n"
+         "  }\n"
+         "  for (int i = KPP_NVAR - 1; i >= 0; i--) {\n"
+         "    const int d = kpp_lu_diag_c[i];\n"
+         "    double x = X[i];\n"
+         "    for (int j = d + 1; j < kpp_lu_crow_c[i + 1]; j++) x = x - JVS[j]*X[kpp_lu_icol_c[j]];\n"
+         "    X[i] = x/JVS[d];\n"
+         "  }\n"
+         "}\n\n";
+  } else {
     std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
     for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
-    // Large mechanisms: the rows in chunks of about kChunkOps operations, one
-    // function each, called in row order (the same operations in the same
-    // order); a single straight-line body of tens of thousands of operations
-    // makes the device assembler's time grow much faster than its length.
-    const bool chunked = m.lu_nonzero >= 2000;
-    const int kChunkOps = 2500;
-    std::vector<int> starts = {0};
-    if (chunked) {
-      int acc = 0;
-      for (int k = 0; k < nvar; k++) {
-        int row_ops = 0;
-        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
-          int j = m.lu_icol[kk];
-          row_ops += 1 + 2 * (m.lu_crow[j + 1] - m.lu_diag[j] - 1);
-        }
-        if (acc > 0 && acc + row_ops > kChunkOps) {
-          starts.push_back(k);
-          acc = 0;
-        }
-        acc += row_ops;
-      }
-    }
-    starts.push_back(nvar);
-    const int nchunks = (int)starts.size() - 1;
-    for (int c = 0; c < nchunks; c++) {
-      if (nchunks > 1)
-        o << "// Rows " << starts[c] << ".." << starts[c + 1] - 1 << " of the LU.\n"
-          << "template <class TJ>\n"
-          << "__device__ __noinline__ int kpp_decomp_rows" << c << "(TJ& JVS) {\n";
-      else
-        o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
-             "// entry of row k is zero on entry to its elimination, 0 on success.\n"
-             "template <class TJ>\n"
-             "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS) {\n";
-      o << "  double a;\n";
-      for (int k = starts[c]; k < starts[c + 1]; k++) {
-        o << "  if (JVS[" << m.lu_diag[k] << "] == 0.0) return " << (k + 1) << ";\n";
-        for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
-          int j = m.lu_icol[kk];
-          ops_decomp += 1;
-          o << "  a = -JVS[" << kk << "] / JVS[" << m.lu_diag[j] << "];\n";
-          o << "  JVS[" << kk << "] = -a;\n";
-          for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
-            int t = pos[k][m.lu_icol[jj]];
-            ops_decomp += 2;
-            o << "  JVS[" << t << "] = JVS[" << t << "] + a*JVS[" << jj << "];\n";
-          }
+    o << "// In-place no-pivot sparse LU of one cell (KppDecomp, util/sutil.c:2-23,\n"
+         "// unrolled in its operation order); returns k+1 when the diagonal entry of\n"
+         "// row k is zero on entry to its elimination, 0 on success.  W (a work row\n"
+         "// for the loop form of large mechanisms) is not used.\n"
+         "template <class TJ, class TW>\n"
+         "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS, TW& W) {\n"
+         "  (void)W;\n"
+         "  double a;\n";
+    for (int k = 0; k < nvar; k++) {
+      o << "  if (JVS[" << m.lu_diag[k] << "] == 0.0) return " << (k + 1) << ";\n";
+      for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
+        int j = m.lu_icol[kk];
+        ops_decomp += 1;
+        o << "  a = -JVS[" << kk << "] / JVS[" << m.lu_diag[j] << "];\n";
+        o << "  JVS[" << kk << "] = -a;\n";
+        for (int jj = m.lu_diag[j] + 1; jj < m.lu_crow[j + 1]; jj++) {
+          int t = pos[k][m.lu_icol[jj]];
+          ops_decomp += 2;
+          o << "  JVS[" << t << "] = JVS[" << t << "] + a*JVS[" << jj << "];\n";
         }
       }
-      o << "  (void)a;\n  return 0;\n}\n\n";
     }
-    if (nchunks > 1) {
-      o << "// In-place no-pivot sparse LU of one cell; returns k+1 when the diagonal\n"
-           "// entry of row k is zero on entry to its elimination, 0 on success.\n"
-           "template <class TJ>\n"
-           "__device__ KPP_MECH_INLINE int kpp_decomp(TJ& JVS) {\n"
-           "  int r;\n";
-      for (int c = 0; c < nchunks; c++)
-        o << "  if ((r = kpp_decomp_rows" << c << "(JVS)) != 0) return r;\n";
-      o << "  return 0;\n}\n\n";
-    }
-  }
+    o << "  (void)a;\n  return 0;\n}\n\n";
 
-  // ---- KppSolve, unrolled
-  o << "// Solve (LU) x = b in place, b given in X.\n"
-       "template <class TJ, class TX>\n"
-       "__device__ KPP_MECH_INLINE void kpp_solve(const TJ& JVS, TX& X) {\n";
-  for (int i = 0; i < nvar; i++) {
-    int b = m.lu_crow[i], e = m.lu_diag[i];
-    if (b < e) {
+    // ---- KppSolve, unrolled
+    o << "// Solve (LU) x = b in place, b given in X.\n"
+         "template <class TJ, class TX>\n"
+         "__device__ KPP_MECH_INLINE void kpp_solve(const TJ& JVS, TX& X) {\n";
+    for (int i = 0; i < nvar; i++) {
+      int b = m.lu_crow[i], e = m.lu_diag[i];
+      if (b < e) {
+        P sum = leaf("X[" + std::to_string(i) + "]");
+        for (int j = b; j < e; j++)
+          sum = sub(sum, mul(leaf("JVS[" + std::to_string(j) + "]"),
+                             leaf("X[" + std::to_string(m.lu_icol[j]) + "]")));
+        ops_solve += count_ops(sum);
+        o << "  X[" << i << "] = " << print(sum) << ";\n";
+      }
+    }
+    for (int i = nvar - 1; i >= 0; i--) {
       P sum = leaf("X[" + std::to_string(i) + "]");
-      for (int j = b; j < e; j++)
+      for (int j = m.lu_diag[i] + 1; j < m.lu_crow[i + 1]; j++)
         sum = sub(sum, mul(leaf("JVS[" + std::to_string(j) + "]"),
                            leaf("X[" + std::to_string(m.lu_icol[j]) + "]")));
+      sum = divide(sum, leaf("JVS[" + std::to_string(m.lu_diag[i]) + "]"));
       ops_solve += count_ops(sum);
       o << "  X[" << i << "] = " << print(sum) << ";\n";
     }
+    o << "}\n\n";
   }
-  for (int i = nvar - 1; i >= 0; i--) {
-    P sum = leaf("X[" + std::to_string(i) + "]");
-    for (int j = m.lu_diag[i] + 1; j < m.lu_crow[i + 1]; j++)
-      sum = sub(sum, mul(leaf("JVS[" + std::to_string(j) + "]"),
-                         leaf("X[" + std::to_string(m.lu_icol[j]) + "]")));
-    sum = divide(sum, leaf("JVS[" + std::to_string(m.lu_diag[i]) + "]"));
-    ops_solve += count_ops(sum);
-    o << "  X[" << i << "] = " << print(sum) << ";\n";
-  }
-  o << "}\n\n";
 
   // ---- KppDecompCmplxR / KppSolveCmplxR (util/sutil.c:28-90), unrolled.
   // The reference runs these generic loops over LU_CROW / LU_ICOL / LU_DIAG
@@ -879,19 +1178,12 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   // performs the same operations on the same values.
   long ops_decomp_c = 0, ops_solve_c = 0;
   std::ostringstream oc;  // written to <prefix>_cmplx.cuh
-  if (m.lu_nonzero >= 2000) {
+  if (m.lu_nonzero >= kGenericLu) {
     // Large patterns: the generic loops over the LU tables, with the dense
     // work row of the reference (the unrolled form would take another long
     // device compile); the same operations in the same order.
-    auto table = [&](const char* name, const std::vector<int>& v) {
-      oc << "__constant__ int " << name << "[" << v.size() << "] = {";
-      for (size_t i = 0; i < v.size(); i++) oc << (i % 16 == 0 ? "\n    " : " ") << v[i] << ",";
-      oc << "};\n";
-    };
+    // the LU tables of the mechanism header (kpp_lu_*_c, the real LU's loop form)
     oc << "#define KPP_CMPLX_GENERIC 1\n";
-    table("kpp_cx_crow", m.lu_crow);
-    table("kpp_cx_diag", m.lu_diag);
-    table("kpp_cx_icol", m.lu_icol);
     for (int k = 0; k < nvar; k++)
       for (int kk = m.lu_crow[k]; kk < m.lu_diag[k]; kk++) {
         const int j = m.lu_icol[kk];
@@ -906,29 +1198,29 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
        "template <class TJ, class TW>\n"
        "__device__ __noinline__ int kpp_decomp_cmplx_w(TJ& JR, TJ& JI, TW& WR, TW& WI) {\n"
        "  for (int k = 0; k < KPP_NVAR; k++) {\n"
-       "    const int dk = kpp_cx_diag[k], b = kpp_cx_crow[k], e = kpp_cx_crow[k + 1];\n"
+       "    const int dk = kpp_lu_diag_c[k], b = kpp_lu_crow_c[k], e = kpp_lu_crow_c[k + 1];\n"
        "    if (JR[dk] == 0.0) return k + 1;\n"
        "    if (JI[dk] == 0.0) return k + 1;\n"
        "    for (int kk = b; kk < e; kk++) {\n"
-       "      WR[kpp_cx_icol[kk]] = JR[kk];\n"
-       "      WI[kpp_cx_icol[kk]] = JI[kk];\n"
+       "      WR[kpp_lu_icol_c[kk]] = JR[kk];\n"
+       "      WI[kpp_lu_icol_c[kk]] = JI[kk];\n"
        "    }\n"
        "    for (int kk = b; kk < dk; kk++) {\n"
-       "      const int j = kpp_cx_icol[kk], dj = kpp_cx_diag[j];\n"
+       "      const int j = kpp_lu_icol_c[kk], dj = kpp_lu_diag_c[j];\n"
        "      const double den = JR[dj]*JR[dj] + JI[dj]*JI[dj];\n"
        "      const double ar = -(WR[j]*JR[dj] + WI[j]*JI[dj])/den;\n"
        "      const double ai = -(WI[j]*JR[dj] - WR[j]*JI[dj])/den;\n"
        "      WR[j] = -ar;\n"
        "      WI[j] = -ai;\n"
-       "      for (int jj = dj + 1; jj < kpp_cx_crow[j + 1]; jj++) {\n"
-       "        const int c = kpp_cx_icol[jj];\n"
+       "      for (int jj = dj + 1; jj < kpp_lu_crow_c[j + 1]; jj++) {\n"
+       "        const int c = kpp_lu_icol_c[jj];\n"
        "        WR[c] = WR[c] + ar*JR[jj] - ai*JI[jj];\n"
        "        WI[c] = WI[c] + ar*JI[jj] + ai*JR[jj];\n"
        "      }\n"
        "    }\n"
        "    for (int kk = b; kk < e; kk++) {\n"
-       "      JR[kk] = WR[kpp_cx_icol[kk]];\n"
-       "      JI[kk] = WI[kpp_cx_icol[kk]];\n"
+       "      JR[kk] = WR[kpp_lu_icol_c[kk]];\n"
+       "      JI[kk] = WI[kpp_lu_icol_c[kk]];\n"
        "    }\n"
        "  }\n"
        "  return 0;\n"
@@ -938,16 +1230,16 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
        "template <class TJ, class TX>\n"
        "__device__ __noinline__ void kpp_solve_cmplx(const TJ& JR, const TJ& JI, TX& XR, TX& XI) {\n"
        "  for (int i = 0; i < KPP_NVAR; i++)\n"
-       "    for (int j = kpp_cx_crow[i]; j < kpp_cx_diag[i]; j++) {\n"
-       "      const int c = kpp_cx_icol[j];\n"
+       "    for (int j = kpp_lu_crow_c[i]; j < kpp_lu_diag_c[i]; j++) {\n"
+       "      const int c = kpp_lu_icol_c[j];\n"
        "      XR[i] = XR[i] - (JR[j]*XR[c] - JI[j]*XI[c]);\n"
        "      XI[i] = XI[i] - (JR[j]*XI[c] + JI[j]*XR[c]);\n"
        "    }\n"
        "  for (int i = KPP_NVAR - 1; i >= 0; i--) {\n"
-       "    const int d = kpp_cx_diag[i];\n"
+       "    const int d = kpp_lu_diag_c[i];\n"
        "    double sumr = XR[i], sumi = XI[i];\n"
-       "    for (int j = d + 1; j < kpp_cx_crow[i + 1]; j++) {\n"
-       "      const int c = kpp_cx_icol[j];\n"
+       "    for (int j = d + 1; j < kpp_lu_crow_c[i + 1]; j++) {\n"
+       "      const int c = kpp_lu_icol_c[j];\n"
        "      sumr = sumr - (JR[j]*XR[c] - JI[j]*XI[c]);\n"
        "      sumi = sumi - (JR[j]*XI[c] + JI[j]*XR[c]);\n"
        "    }\n"
@@ -1034,7 +1326,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   oc << "#define KPP_OPS_DECOMP_CMPLX " << ops_decomp_c << "\n"
      << "#define KPP_OPS_SOLVE_CMPLX " << ops_solve_c << "\n";
 
-  emit_warp_tables(o, m);
+  emit_coop_tables(o, m);
 
   std::ofstream f(out_prefix + ".cuh");
   if (!f) return false;

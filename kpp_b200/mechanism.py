@@ -195,6 +195,47 @@ class Mechanism:
             raise KppError(f"{name} must be a contiguous {dtype} tensor")
         return t
 
+    def _shapes(self, ld: int, n: int, rows=(), cols=(), device=None, tol=None, vector_tol=False):
+        """Shapes the C ABI reads or writes, checked before the call so that a
+        wrong shape is a KppError rather than an out-of-bounds device access.
+        rows: (tensor, name, nrows) that must be [nrows, ld] (the ABI's leading
+        dimension is ld for every batched 2-D array); cols: (tensor, name) 1-D
+        arrays indexed by cell, at least n entries; tol: (atol, rtol), NVAR
+        entries with vector tolerances, else 1; every tensor on `device`."""
+        if not 0 <= n <= ld:
+            raise KppError(f"ncells must be in [0, ld]: ncells={n}, ld={ld}")
+        allt = []
+        for t, nm, nr in rows:
+            if t is None:
+                continue
+            if t.dim() != 2 or t.shape[0] != nr or t.shape[1] != ld:
+                raise KppError(f"{nm} must have shape [{nr}, {ld}], got {list(t.shape)}")
+            allt.append((t, nm))
+        for t, nm in cols:
+            if t is None:
+                continue
+            if t.dim() != 1 or t.shape[0] < n:
+                raise KppError(f"{nm} must be 1-D with at least {n} entries, got {list(t.shape)}")
+            allt.append((t, nm))
+        if tol is not None:
+            need = self.nvar if vector_tol else 1
+            for t, nm in zip(tol, ("atol", "rtol")):
+                if t is None or t.numel() < need:
+                    raise KppError(f"{nm} needs at least {need} entries")
+                allt.append((t, nm))
+        if device is not None:
+            for t, nm in allt:
+                if t.device != device:
+                    raise KppError(f"{nm} is on {t.device}, expected {device}")
+
+    def _outputs(self, out, ld, rstatus_rows, device):
+        if out is not None:
+            self._shapes(ld, ld, rows=((out.istatus, "out.istatus", 8),
+                                       (out.rstatus, "out.rstatus", rstatus_rows)),
+                         cols=((out.ierr, "out.ierr"),), device=device)
+            if out.ierr.shape[0] != ld:
+                raise KppError(f"out.ierr must have {ld} entries")
+
     def rosenbrock(self, var: torch.Tensor, fix: torch.Tensor, temp: torch.Tensor,
                    tstart: torch.Tensor, tend: torch.Tensor, atol: torch.Tensor,
                    rtol: torch.Tensor, ipar: Sequence[int], rpar: Sequence[float],
@@ -213,6 +254,11 @@ class Mechanism:
                       (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun"),
                       (hstart, "hstart")):
             self._dev(t, f64, nm)
+        self._shapes(ld, n, rows=((var, "var", self.nvar), (fix, "fix", self.nfix)),
+                     cols=((temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                           (cfactor, "cfactor"), (sun, "sun"), (hstart, "hstart")),
+                     device=var.device, tol=(atol, rtol), vector_tol=int(ipar[1]) == 0)
+        self._outputs(out, ld, 2, var.device)
         if out is None:
             out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
                                    istatus=torch.empty(8, ld, dtype=i32, device=var.device),
@@ -247,6 +293,11 @@ class Mechanism:
         for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
                       (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun")):
             self._dev(t, f64, nm)
+        self._shapes(ld, n, rows=((var, "var", self.nvar), (fix, "fix", self.nfix)),
+                     cols=((temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                           (cfactor, "cfactor"), (sun, "sun")),
+                     device=var.device, tol=(atol, rtol), vector_tol=int(icntrl[1]) == 0)
+        self._outputs(out, ld, 3, var.device)
         if out is None:
             out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
                                    istatus=torch.empty(8, ld, dtype=i32, device=var.device),
@@ -276,6 +327,11 @@ class Mechanism:
         for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
                       (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun")):
             self._dev(t, f64, nm)
+        self._shapes(ld, n, rows=((var, "var", self.nvar), (fix, "fix", self.nfix)),
+                     cols=((temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                           (cfactor, "cfactor"), (sun, "sun")),
+                     device=var.device, tol=(atol, rtol), vector_tol=int(icntrl[1]) == 0)
+        self._outputs(out, ld, 3, var.device)
         if out is None:
             out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
                                    istatus=torch.empty(8, ld, dtype=i32, device=var.device),
@@ -310,6 +366,11 @@ class Mechanism:
                       (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun"), (hstart, "hstart")):
             self._dev(t, f64, nm)
         self._dev(order, i32, "order")
+        self._shapes(ld, n, rows=((var, "var", self.nvar), (fix, "fix", self.nfix)),
+                     cols=((temp, "temp"), (tstart, "tstart"), (cfactor, "cfactor"),
+                           (sun, "sun"), (hstart, "hstart"), (order, "order")),
+                     device=var.device, tol=(atol, rtol), vector_tol=int(ipar[1]) == 0)
+        self._outputs(out, ld, 2, var.device)
         if out is None:
             out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
                                    istatus=torch.empty(8, ld, dtype=i32, device=var.device),
@@ -403,8 +464,12 @@ class Mechanism:
         """Batched Update_RCONST / Fun / Jac_SP at one time (kpp_b200_fun_jac)."""
         f64 = torch.float64
         self._dev(var, f64, "var")
+        for t, nm in ((fix, "fix"), (temp, "temp"), (cfactor, "cfactor"), (sun, "sun")):
+            self._dev(t, f64, nm)
         ld = var.shape[1]
         dev = var.device
+        self._shapes(ld, ld, rows=((var, "var", self.nvar), (fix, "fix", self.nfix)),
+                     cols=((temp, "temp"), (cfactor, "cfactor"), (sun, "sun")), device=dev)
         rconst = torch.empty(self.nreact, ld, dtype=f64, device=dev) if "rconst" in want else None
         vdot = torch.empty(self.nvar, ld, dtype=f64, device=dev) if "vdot" in want else None
         jvs = torch.empty(self.lu_nonzero, ld, dtype=f64, device=dev) if "jvs" in want else None
@@ -418,7 +483,10 @@ class Mechanism:
     def decomp_solve(self, jvs: torch.Tensor, x: Optional[torch.Tensor] = None, stream=None):
         """In-place batched KppDecomp (+ KppSolve of x); returns ising [ld]."""
         self._dev(jvs, torch.float64, "jvs")
+        self._dev(x, torch.float64, "x")
         ld = jvs.shape[1]
+        self._shapes(ld, ld, rows=((jvs, "jvs", self.lu_nonzero), (x, "x", self.nvar)),
+                     device=jvs.device)
         ising = torch.empty(ld, dtype=torch.int32, device=jvs.device)
         s = stream if stream is not None else torch.cuda.current_stream(jvs.device)
         self._check(self.lib.kpp_b200_decomp_solve(ld, ld, _ptr(jvs), _ptr(x), _ptr(ising),
@@ -431,7 +499,10 @@ class Mechanism:
         with jvs [LU_NONZERO, ld] and uv [NVAR, ld]."""
         self._dev(jvs, torch.float64, "jvs")
         self._dev(uv, torch.float64, "uv")
+        self._dev(out, torch.float64, "out")
         ld = jvs.shape[1]
+        self._shapes(ld, ld, rows=((jvs, "jvs", self.lu_nonzero), (uv, "uv", self.nvar),
+                                   (out, "out", self.nvar)), device=jvs.device)
         if out is None:
             out = torch.empty_like(uv)
         s = stream if stream is not None else torch.cuda.current_stream(jvs.device)
@@ -445,7 +516,10 @@ class Mechanism:
         KppSolveTR)."""
         self._dev(jvs, torch.float64, "jvs")
         self._dev(x, torch.float64, "x")
+        self._dev(out, torch.float64, "out")
         ld = jvs.shape[1]
+        self._shapes(ld, ld, rows=((jvs, "jvs", self.lu_nonzero), (x, "x", self.nvar),
+                                   (out, "out", self.nvar)), device=jvs.device)
         if out is None:
             out = torch.empty_like(x)
         s = stream if stream is not None else torch.cuda.current_stream(jvs.device)

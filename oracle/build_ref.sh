@@ -37,6 +37,8 @@ fi
 
 CC="${CC:-gcc}"
 mkdir -p "$OUT/obj"
+# the source tree the tests read the reference's mechanisms from
+echo "$KPP_REF" > "$OUT/kpp_home"
 
 # ---- 1. the generator -------------------------------------------------------
 GEN_SRCS=(code code_c code_f77 code_f90 code_matlab debug gen kpp scanner scanutil)

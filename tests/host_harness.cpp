@@ -9,6 +9,7 @@
 #define __host__
 #define __forceinline__ inline
 #define __noinline__
+#define __constant__
 #include <cmath>
 using std::cos;
 using std::exp;
@@ -44,7 +45,10 @@ void host_jac(const double* var, const double* fix, const double* rconst, double
   kpp_jac_sp<false>(var, fix, rconst, jvs, b);
 }
 
-int host_decomp(double* jvs) { return kpp_decomp(jvs); }
+int host_decomp(double* jvs) {
+  double w[KPP_NVAR];  // work row of the loop-form LU of large mechanisms
+  return kpp_decomp(jvs, w);
+}
 
 void host_solve(const double* jvs, double* x) { kpp_solve(jvs, x); }
 

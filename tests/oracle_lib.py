@@ -12,6 +12,7 @@ cell index fastest).
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -20,6 +21,16 @@ import numpy as np
 REPO = Path(__file__).resolve().parents[1]
 REF_DIR = REPO / "oracle" / "_ref"
 _vp = ctypes.c_void_p
+
+
+def kpp_home() -> str:
+    """KPP's source tree: $KPP_HOME, else the tree the oracle was last built
+    from (recorded by oracle/build_ref.sh), else empty."""
+    home = os.environ.get("KPP_HOME", "")
+    if home:
+        return home
+    rec = REF_DIR / "kpp_home"
+    return rec.read_text().strip() if rec.exists() else ""
 
 
 def lib_path(mech: str, opt: str = "") -> Path:

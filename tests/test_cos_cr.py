@@ -1,5 +1,7 @@
 """The correctly rounded cosine used by the device Update_SUN (CPU): compiled
-for the host from the same source, checked against 200-bit mpmath."""
+for the host from the same source, it must equal the correctly rounded cosine
+(mpmath at 200 bits, rounded to double) exactly -- an error bound of 0.5 ulp --
+on 20000 seeded arguments of Update_SUN's range [-pi, pi] and its end points."""
 import ctypes
 import math
 import shutil

@@ -63,3 +63,14 @@ def test_jacobian_products_and_transposed_solve_bit_identical(mech, golden_dir):
         want = np.zeros(o.nvar)
         ref.KppSolveTR(_p(ec), _p(xc), _p(want))
         np.testing.assert_array_equal(got[:, c], want)
+    # in place, as the reference's adjoint integrators call it
+    # (KppSolveTR(A, b, b)): the output aliases the right-hand side
+    xd = d(x)
+    got_in_place = m.solve_tr(d(e), xd, out=xd).cpu().numpy()
+    for c in range(n):
+        if not ok[c]:
+            continue
+        ec = np.ascontiguousarray(e[:, c])
+        xc = np.ascontiguousarray(x[:, c])
+        ref.KppSolveTR(_p(ec), _p(xc), _p(xc))
+        np.testing.assert_array_equal(got_in_place[:, c], xc)

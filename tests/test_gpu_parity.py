@@ -124,7 +124,9 @@ def test_integrate_matches_live_reference(mech, ncells, nsteps):
         hstart = r.rstatus[1].clone()
         torch.cuda.synchronize()
         np.testing.assert_array_equal(r.ierr.cpu().numpy(), ierr)
-        assert_var_parity(var.cpu().numpy(), var_ref, var_alt, f"step {k}")
+        # saprc99, the benchmark mechanism, needs no rounding envelope at all
+        assert_var_parity(var.cpu().numpy(), var_ref, var_alt, f"step {k}",
+                          **({"max_env_fraction": 0.0} if mech == "saprc99" else {}))
         assert np.all(r.istatus.cpu().numpy() == ist, axis=0).mean() >= 0.95
         # continue both chains from the reference state so each step is compared
         # from identical inputs

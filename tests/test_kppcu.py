@@ -19,10 +19,10 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from oracle_lib import OracleLib, REPO, ensure_built
+from oracle_lib import OracleLib, REPO, ensure_built, kpp_home
 
 BUILD = REPO / "kpp_b200" / "_build"
-KPP_HOME = os.environ.get("KPP_HOME", "/root/reference")
+KPP_HOME = kpp_home()
 HAVE_SOURCES = (Path(KPP_HOME) / "models" / "small_strato.eqn").exists()
 MECHS = ["small_strato", "saprc99"]
 
