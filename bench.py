@@ -278,6 +278,27 @@ def tight_reference(wl, cells, pool):
     return np.concatenate([r[0] for r in res], axis=1), np.concatenate([r[1] for r in res])
 
 
+def tight_gpu(mech, wl, cells, dev):
+    """The same FP64 Rodas4 RTOL 1e-10 solution as tight_reference, for the
+    given cells, by the library's own integrator (whose parity with the
+    reference the tests establish); returns (var, ierr, ms)."""
+    import torch
+    from kpp_b200.controls import make_controls
+    ipar, rpar = make_controls(method="rodas4", scalar_tol=True, max_steps=1_000_000)
+    D = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    t0, t1 = wl.step_bounds(0)
+    var = D(wl.var[:, cells])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r = mech.rosenbrock(var, D(wl.fix[:, cells]), D(wl.temp[cells]), D(t0[cells]), D(t1[cells]),
+                        D(np.array([TIGHT_ATOL])), D(np.array([TIGHT_RTOL])), ipar, rpar,
+                        cfactor=None if wl.cfactor is None else D(wl.cfactor[cells]),
+                        sun=None if wl.sun is None else D(wl.sun[cells]))
+    e1.record()
+    torch.cuda.synchronize()
+    return var.cpu().numpy(), r.ierr.cpu().numpy(), e0.elapsed_time(e1)
+
+
 def accuracy(got: np.ndarray, ref: np.ndarray, atol: float, rtol: float) -> dict:
     """Error of an RTOL 1e-3 solution against the tight one: the largest
     relative error over species above 1e3 ATOL (where the relative tolerance
@@ -300,6 +321,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
     mech.set_kernel(args.kernel)
+    mech.set_queue_lanes(args.queue == "lanes")
     shape = None
     if args.kernel == "auto":
         from kpp_b200 import autotune
@@ -339,11 +361,15 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
 
     class Arm:
         """One way of running the steps: plain (grid-stride kernel, Hstart =
-        STEPMIN) or learned (plan, then the work-queue kernel in cost order
-        with the planned Hstart)."""
+        STEPMIN), learned (plan, then the work-queue kernel in cost order
+        with the planned Hstart) or, with `fixed` = (Hstart, order) tensors,
+        the work-queue kernel with a given Hstart and order (the ceiling arm:
+        each cell's best starting step among the training candidates, queued
+        by its true step count)."""
 
-        def __init__(self, learned):
+        def __init__(self, learned, fixed=None):
             self.learned = learned
+            self.fixed = fixed
             self.out = None
             self.hs = torch.zeros(n, dtype=torch.float64, device=dev)
             self.hs_plan = torch.empty(n, dtype=torch.float64, device=dev)
@@ -359,7 +385,13 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             t0, t1 = t_bounds[kk]
             warm = None if fresh else self.hs
             ev = self.kernel_events[k] if self.kernel_events else None
-            if not self.learned:
+            if self.fixed is not None:
+                if ev:
+                    ev[0].record(stream)
+                self.out = mech.rosenbrock_chain(
+                    var, fix, temp, t0, wl.dt, 1, atol, rtol, wl.ipar, wl.rpar, cfactor=cf,
+                    sun=sun, hstart=self.fixed[0], order=self.fixed[1], out=self.out)
+            elif not self.learned:
                 if ev:
                     ev[0].record(stream)
                 self.out = mech.rosenbrock(var, fix, temp, t0, t1, atol, rtol, wl.ipar, wl.rpar,
@@ -425,6 +457,29 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     plain = Arm(False).run()
     learned = Arm(True).run() if sched is not None else None
     head = learned if learned is not None else plain
+    # the ceiling of a starting step plus cost order on this workload: every
+    # cell integrated once per training candidate Hstart (the plain
+    # integrator), then timed with its best candidate, queued by the step
+    # count that candidate took
+    ceiling, ceiling_info = None, None
+    if args.ceiling and fresh and learned is not None:
+        from kpp_b200 import scheduler as _sch
+        t_c = time.perf_counter()
+        nstp_c, ok_c = _sch.log_tuples(mech, wl, verbose=False)
+        best = np.argmin(nstp_c, axis=0)
+        cols = np.arange(n)
+        hs_best = np.asarray(_sch.CANDIDATES)[best]
+        cost = nstp_c[best, cols]
+        order_best = np.argsort(-cost, kind="stable").astype(np.int32)
+        ceiling = Arm(False, fixed=(D(hs_best), D(order_best))).run()
+        ceiling_info = {
+            "what": "each cell's best Hstart among the 9 training candidates (1e-6 .. 1e-2 s, "
+                    "half decades), queue sorted by the step count it took (decreasing)",
+            "candidates_s": list(_sch.CANDIDATES),
+            "mean_nstp_default_hstart": float(plain.ist[2] / (n * args.steps)),
+            "mean_nstp_best_candidate": float(cost.mean()),
+            "tuple_logging_s": time.perf_counter() - t_c,
+            "ierr_identical_to_plain": bool(np.array_equal(ceiling.ierr, plain.ierr))}
 
     from kpp_b200.controls import METHODS
     method_name = {v: k for k, v in METHODS.items()}[wl.ipar[3]]
@@ -555,6 +610,10 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             "speedup_vs_plain": learned.value / plain.value,
             "plan_ms": e0.elapsed_time(e1) / 3,
             "ierr_identical_to_plain": bool(np.array_equal(learned.ierr, plain.ierr)),
+            "ceiling": None if ceiling is None else dict(
+                ceiling_info, value=ceiling.value, speedup_vs_plain=ceiling.value / plain.value,
+                learned_fraction_of_ceiling=learned.value / ceiling.value,
+                stats=ceiling.summary()),
             "network": "78 features -> 3 x 256 GELU -> 2 (log10 Hstart, ln Nstp); BF16 "
                        "mma.sync GEMMs, FP32 accumulate; trained on the GPU by "
                        "kpp_b200.train_scheduler",
@@ -565,17 +624,41 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         })
     elif sched_note:
         sched_block["note"] = sched_note
-    if pool is not None and fresh and args.accuracy_cells > 0:
-        cells = np.linspace(0, n - 1, args.accuracy_cells).astype(np.int64)
-        ref, ref_ierr = tight_reference(wl, cells, pool)
+    if fresh and args.accuracy_cells > 0:
+        # cells spread over every cost level: evenly spaced positions of the
+        # queue order by cost (the learned plan's order), else of the batch
+        if learned is not None:
+            sched.plan(var0, temp, t_bounds[0][0], cfactor=cf, sun=sun, tend=t_bounds[0][1],
+                       hstart=torch.empty(n, dtype=torch.float64, device=dev),
+                       order=(order_acc := torch.empty(n, dtype=torch.int32, device=dev)))
+            pick = order_acc.cpu().numpy()
+        else:
+            pick = np.arange(n)
+        cells = np.sort(pick[np.linspace(0, n - 1, min(args.accuracy_cells, n)).astype(np.int64)])
+        ref, ref_ierr, tight_ms = tight_gpu(mech, wl, cells, dev)
         ok = ref_ierr == 1  # cells the tight solve finished
-        acc = {"plain": accuracy(plain.var_out[:, cells[ok]], ref[:, ok], float(wl.atol[0]),
-                                 float(wl.rtol[0])) if ok.any() else None,
+        A = lambda arm: accuracy(arm.var_out[:, cells[ok]], ref[:, ok], float(wl.atol[0]),
+                                 float(wl.rtol[0])) if arm is not None and ok.any() else None
+        acc = {"plain": A(plain), "learned": A(learned), "ceiling": A(ceiling),
+               "oracle": f"FP64 Rodas4, RTOL {TIGHT_RTOL:g}, ATOL {TIGHT_ATOL:g}, at most 10^6 "
+                         f"steps, on the GPU ({tight_ms / 1e3:.1f} s); cells evenly spaced "
+                         f"over the cost order",
                "oracle_cells_ok": int(ok.sum()), "oracle_cells": int(ok.size),
                "oracle_ierr": sorted(set(int(x) for x in ref_ierr))}
-        if learned is not None and ok.any():
-            acc["learned"] = accuracy(learned.var_out[:, cells[ok]], ref[:, ok],
-                                      float(wl.atol[0]), float(wl.rtol[0]))
+        if pool is not None and args.accuracy_cpu_cells > 0:
+            # the tight GPU solution against the CPU restatement of the
+            # reference Rosenbrock on a subset of those cells
+            sub = cells[np.linspace(0, len(cells) - 1, args.accuracy_cpu_cells).astype(np.int64)]
+            cpu_ref, cpu_ierr = tight_reference(wl, sub, pool)
+            idx = np.searchsorted(cells, sub)
+            both = (cpu_ierr == 1) & ok[idx]
+            if both.any():
+                g, c = ref[:, idx[both]], cpu_ref[:, both]
+                mask = np.abs(c) > 1e3 * TIGHT_ATOL
+                acc["oracle_gpu_vs_cpu"] = {
+                    "cells": int(both.sum()),
+                    "max_rel_diff_above_1e3_atol": float((np.abs(g - c)[mask] / np.abs(c)[mask]).max())
+                    if mask.any() else None}
         sched_block["accuracy_vs_fp64_rtol1e-10"] = acc
 
     nchunks = (n + (1 << 17) - 1) >> 17
@@ -591,6 +674,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                                f"{wl.rtol[0]:g} ATOL {wl.atol[0]:g}",
                    "mode": args.mode, "cells_per_gpu": n, "chemistry_step_s": wl.dt,
                    "method": method_name, "scheduler": sched_block["kind"],
+                   "queue": args.queue,
                    "parallelism": f"cell shards x{world}",
                    "kernel": {"thread": "thread per cell", "warp": "warp per cell"}[kernel],
                    "launch_shape": shape or {"kernel": kernel, "blocks_per_sm": 0,
@@ -986,9 +1070,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--kernel", choices=["auto", "thread", "warp"], default="auto")
+    ap.add_argument("--queue", choices=["lanes", "warps"], default="lanes",
+                    help="work-queue granularity of the learned and ceiling arms: each lane "
+                         "takes one cell at a time, or each warp 32")
     ap.add_argument("--scheduler", choices=["learned", "plain"], default="learned")
     ap.add_argument("--weights", default=None, help="trained scheduler (.npz)")
-    ap.add_argument("--accuracy-cells", type=int, default=64)
+    ap.add_argument("--accuracy-cells", type=int, default=4096,
+                    help="cells compared with the FP64 RTOL 1e-10 solution (on the GPU)")
+    ap.add_argument("--accuracy-cpu-cells", type=int, default=64,
+                    help="of those, cells also solved by the CPU oracle as a cross-check")
+    ap.add_argument("--no-ceiling", dest="ceiling", action="store_false",
+                    help="skip the ceiling arm (best starting step, true cost order)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

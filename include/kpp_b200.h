@@ -284,13 +284,35 @@ int kpp_b200_decomp_solve(int ncells, int ld, double *jvs, double *x,
 
 /* Kernel used by the Rosenbrock entries (process-wide): 0 automatic (the
  * default), 1 one thread per cell with the work set in device memory, 2 one
- * warp per cell with the work set in shared memory (mechanisms whose work set
- * is in device memory and fits shared memory; others keep kernel 1).  Both
- * kernels give bit-identical results.  Automatic selects kernel 1.  No
- * counterpart in the reference.
- * kpp_b200_get_kernel returns the kernel in effect (1 or 2). */
+ * warp per cell with the work set in shared memory (the mechanism's schedule
+ * tables staged in shared memory once per CTA; no work buffer).  Kernel 2 runs
+ * the launches whose rate constants are fixed for the call (SUN given per
+ * cell, or no SUN-dependent rates; no rates of time or concentrations) of
+ * mechanisms with at most 1024 LU entries; other launches use kernel 1.  Both
+ * kernels give bit-identical results.  Automatic selects kernel 2 for such
+ * launches of at most kpp_b200_get_auto_warp_cells() cells and kernel 1
+ * otherwise: the thread-per-cell kernel needs about 150k cells to fill a
+ * B200, the warp-per-cell kernel 1776.  No counterpart in the reference.
+ * kpp_b200_get_kernel returns the configured kernel (1 or 2; 1 for
+ * automatic). */
 int kpp_b200_set_kernel(int which);
 int kpp_b200_get_kernel(void);
+
+/* Work-queue granularity of kpp_b200_rosenbrock_chain on the thread-per-cell
+ * kernel (process-wide): 0 (the default) each warp takes the next 32 queue
+ * positions and its lanes start every chained call together; 1 each lane
+ * takes the next single position as soon as its previous cell is done, so no
+ * lane idles until the slowest cell of its warp finishes.  Results do not
+ * depend on it.  No counterpart in the reference. */
+int kpp_b200_set_queue_lanes(int per_lane);
+int kpp_b200_get_queue_lanes(void);
+
+/* The automatic choice's limit (process-wide): launches of at most `ncells`
+ * cells use the warp-per-cell kernel when they can (0: never).  The autotuner
+ * (kpp_b200/autotune.py) measures the crossing point per device and
+ * mechanism.  No counterpart in the reference. */
+int kpp_b200_set_auto_warp_cells(int ncells);
+int kpp_b200_get_auto_warp_cells(void);
 
 /* Launch shape of the thread-per-cell kernel (process-wide): the number of
  * 128-thread blocks per SM the Rosenbrock entries keep resident, 0 (the

@@ -212,9 +212,10 @@ def build_util(force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     src = CSRC / "kpp_util.cu"
     lib = LIB / "libkpp_b200_util.so"
-    flags = ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-lineinfo"]
+    flags = ARCH + ["-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                    "-lineinfo"]
     stamp = BUILD / "util.stamp"
-    digest = _hash_files([src], " ".join(flags))
+    digest = _hash_files([src, CSRC / "kpp_div.cuh"], " ".join(flags))
     if not force and lib.exists() and stamp.exists() and stamp.read_text() == digest:
         return lib
     _run([nvcc()] + flags + [str(src), "-o", str(lib)])
@@ -241,11 +242,10 @@ def build_sched(force: bool = False) -> Path:
     return lib
 
 
-# Mechanisms whose device code takes long to compile (MCM isoprene: ~20 min of
-# nvcc on 8 cores for 1944 reactions and a 41k-operation LU).  The default
-# build includes them once their library exists (so they stay up to date);
-# `python -m kpp_b200.build --all` or naming one builds it the first time.
-ON_REQUEST = {"mcm_isoprene"}
+# Mechanisms built only when named (`python -m kpp_b200.build <mech>` or
+# `--all`), or once their library exists.  None at present: MCM isoprene's LU
+# and solve are loops over the LU tables (kppcu), so it builds with the rest.
+ON_REQUEST: set = set()
 
 
 def all_mechanisms():

@@ -166,6 +166,7 @@ struct LaunchArgs {
                      // null for the grid-stride loop
   int nchain;        // > 0: that many calls [T, T + chain_dt], T += chain_dt
   double chain_dt;
+  int lane_queue;    // with `queue`: each lane takes one cell at a time
 };
 
 // Whether the warp-per-cell kernel (kpp_coop.cuh) can integrate a launch: the
@@ -184,8 +185,8 @@ struct Stats {
 // its 32 cells issues one coalesced 256-byte access; every access is the
 // lane's block pointer plus a compile-time constant below 1 MB, so it fits
 // the load/store immediate offset, and the compiler can prove that different
-// elements do not alias and keep, reorder and batch its loads.
-constexpr long kSlotStride = 1L << 17;  // thread slots the layout holds (>= resident threads)
+// elements do not alias and keep, reorder and batch its loads.  The layout
+// spans the launch's thread slots in whole warps (scratch_bytes).
 constexpr int kLanes = 32;
 
 struct Strided {

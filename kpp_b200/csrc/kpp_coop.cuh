@@ -31,6 +31,8 @@
 // kernel.
 #pragma once
 
+#include "kpp_div.cuh"
+
 namespace coop {
 
 namespace K = kpp_coop;
@@ -49,10 +51,11 @@ struct Cell {
   static constexpr int V1 = A + K::NA;          // ynew, FIX, 1.0
   static constexpr int FCN = V1 + K::NEXT;      // stage Fun; then Yerr and the error terms
   static constexpr int KS = FCN + NVAR;         // stage vectors
-  static constexpr int END = KS + S * NVAR;
-  // Jac_SP's partial derivatives reuse [FCN, END) (dead while the matrix is
+  static constexpr int RY = KS + S * NVAR;      // reciprocals of the U diagonal
+  static constexpr int END = RY + NVAR;
+  // Jac_SP's partial derivatives reuse [FCN, RY) (dead while the matrix is
   // built) when they fit there
-  static constexpr int B = (END - FCN >= K::NB) ? FCN : END;
+  static constexpr int B = (RY - FCN >= K::NB) ? FCN : END;
   static constexpr int TOTAL = (B == FCN) ? END : END + K::NB;
   static_assert(LU_NZ + K::NA >= NREACT, "rate constants are staged in [JVS, V1)");
 };
@@ -73,10 +76,19 @@ constexpr size_t smem_bytes() {
 
 // ---- phases (all lanes of the warp call each one) ----------------------------
 
+// Every phase below first loads what its lanes need -- table entries, then
+// their operands -- into registers and only then computes, so that each
+// lane's loads overlap instead of forming one long chain of dependent
+// shared-memory round trips.  Within one iteration of a schedule no lane reads
+// what another lane of that iteration writes, and a lane's own entries of one
+// iteration do not depend on each other, so all loads of an iteration can go
+// first.
+
 // Product weights of a lane: round r covers product r*32 + lane.
 template <int R>
-__device__ __forceinline__ void weights(const unsigned* tab, int off, const double* kc,
-                                        const double* rc, double (&w)[R], int lane) {
+__device__ __forceinline__ void weights(const unsigned* __restrict__ tab, int off,
+                                        const double* __restrict__ kc,
+                                        const double* __restrict__ rc, double (&w)[R], int lane) {
   constexpr unsigned RM = (1u << K::RATE_BITS) - 1;
 #pragma unroll
   for (int r = 0; r < R; r++) {
@@ -87,51 +99,74 @@ __device__ __forceinline__ void weights(const unsigned* tab, int off, const doub
   }
 }
 
-// out[t] = weight(t) x the reactant factors of product t, for t < N.
+// out[t] = weight(t) x the reactant factors of product t, for t < N.  The
+// table is padded to whole rounds with the constant 1.0 as every factor.
 template <int R, int N>
-__device__ __forceinline__ void products(const unsigned* tab, int off, const double (&w)[R],
-                                         const double* vext, double* out, int lane) {
+__device__ __forceinline__ void products(const unsigned* __restrict__ tab, int off,
+                                         const double (&w)[R], const double* __restrict__ vext,
+                                         double* __restrict__ out, int lane) {
+  unsigned f[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) f[r] = tab[off + r * 32 + lane];
+  double v[R][K::MAXF];
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int k = 0; k < K::MAXF; k++) v[r][k] = vext[(f[r] >> (8 * k)) & 255u];
 #pragma unroll
   for (int r = 0; r < R; r++) {
-    const int t = r * 32 + lane;
-    if (t < N) {
-      const unsigned f = tab[off + t];
-      double v = w[r];
+    double x = w[r];
 #pragma unroll
-      for (int k = 0; k < K::MAXF; k++) v = v * vext[(f >> (8 * k)) & 255u];
-      out[t] = v;
-    }
+    for (int k = 0; k < K::MAXF; k++) x = x * v[r][k];
+    if (r * 32 + lane < N) out[r * 32 + lane] = x;
   }
 }
 
 // The lane streams of a sum phase: out[dst] = sum of kc[coef] * src[idx] in
 // order, negated for the Rosenbrock matrix (NEG), with 1/(h gamma) added on
-// diagonal entries (DIAG).
+// diagonal entries (DIAG).  Entries are taken in chunks of CH: their table
+// words, then their operands, then the running sums.
 template <int L, bool NEG, bool DIAG>
-__device__ __forceinline__ void sums(const unsigned* tab, int off, const double* kc,
-                                     const double* src, double* out, double ghinv, int lane) {
+__device__ __forceinline__ void sums(const unsigned* __restrict__ tab, int off,
+                                     const double* __restrict__ kc,
+                                     const double* __restrict__ src, double* __restrict__ out,
+                                     double ghinv, int lane) {
   constexpr int SB = K::SUM_SRC_BITS, CB = K::SUM_COEF_BITS, FB = SB + CB;
+  constexpr unsigned SM = (1u << SB) - 1, CM = (1u << CB) - 1;
+  constexpr int CH = 8;
   double acc = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < L; k++) {
-    const unsigned e = tab[off + k * 32 + lane];
-    if (e == kNop) continue;
-    double val;
-    if ((e >> (FB + 2)) & 1u) {
-      val = NEG ? -0.0 : 0.0;
-    } else {
-      const double p = kc[(e >> SB) & ((1u << CB) - 1)] * src[e & ((1u << SB) - 1)];
-      acc = ((e >> FB) & 1u) ? p : acc + p;
-      val = NEG ? -acc : acc;
+#pragma unroll 2
+  for (int k0 = 0; k0 < L; k0 += CH) {
+    unsigned e[CH];
+    double p[CH];
+#pragma unroll
+    for (int j = 0; j < CH; j++) e[j] = (k0 + j < L) ? tab[off + (k0 + j) * 32 + lane] : kNop;
+#pragma unroll
+    for (int j = 0; j < CH; j++) {
+      const unsigned ej = (e[j] == kNop) ? 0u : e[j];  // a NOP reads entry 0's operands
+      p[j] = kc[(ej >> SB) & CM] * src[ej & SM];
     }
-    if ((e >> (FB + 1)) & 1u) {
-      if (DIAG && ((e >> (FB + 3)) & 1u)) val = val + ghinv;
-      out[e >> (FB + 4)] = val;
+#pragma unroll
+    for (int j = 0; j < CH; j++) {
+      const unsigned ej = e[j];
+      if (ej == kNop) continue;
+      double val;
+      if ((ej >> (FB + 2)) & 1u) {
+        val = NEG ? -0.0 : 0.0;
+      } else {
+        acc = ((ej >> FB) & 1u) ? p[j] : acc + p[j];
+        val = NEG ? -acc : acc;
+      }
+      if ((ej >> (FB + 1)) & 1u) {
+        if (DIAG && ((ej >> (FB + 3)) & 1u)) val = val + ghinv;
+        out[ej >> (FB + 4)] = val;
+      }
     }
   }
 }
 
-__device__ __forceinline__ int lane_count(const unsigned* tab, int off, int it, int lane) {
+__device__ __forceinline__ int lane_count(const unsigned* __restrict__ tab, int off, int it,
+                                          int lane) {
   return (tab[off + it * 4 + (lane >> 3)] >> ((lane & 7) * 4)) & 15u;
 }
 
@@ -168,61 +203,96 @@ __device__ __forceinline__ int warp_min(int v) {
 
 // In-place no-pivot sparse LU; returns k+1 for the first row whose diagonal
 // is zero on entry to its elimination (its original value: util/sutil.c only
-// changes a row during that row's own elimination), 0 on success.
-__device__ __forceinline__ int decomp(const unsigned* tab, double* J, int lane) {
+// changes a row during that row's own elimination), 0 on success.  On success
+// ry[i] = 1/U(i,i), the divisors of the backward substitution.
+__device__ __forceinline__ int decomp(const unsigned* __restrict__ tab, double* J, double* ry,
+                                      int lane) {
   int bad = NVAR;
   for (int i = lane; i < NVAR; i += 32)
     if (J[tab[K::O_DIAG + i]] == 0.0 && i < bad) bad = i;
   bad = warp_min(bad);
   if (bad < NVAR) return bad + 1;
-  constexpr int B = K::LU_BITS;
+  constexpr int B = K::LU_BITS, CAP = K::LU_CAP;
   constexpr unsigned M = (1u << B) - 1;
   int pos = 0;
+  int n = lane_count(tab, K::O_CLU, 0, lane);
   for (int it = 0; it < K::IT_LU; it++) {
-    const int n = lane_count(tab, K::O_CLU, it, lane);
-    for (int j = 0; j < n; j++) {
-      const unsigned e = tab[K::O_LU + (pos + j) * 32 + lane];
-      const int t = (e >> (2 * B)) & M, m = (e >> B) & M, s = e & M;
-      if (e >> 31)
-        J[t] = J[t] / J[s];
-      else
-        J[t] = J[t] + (-J[m]) * J[s];
+    unsigned e[CAP];
+    double vt[CAP], vm[CAP], vs[CAP];
+#pragma unroll
+    for (int j = 0; j < CAP; j++) e[j] = (j < n) ? tab[K::O_LU + (pos + j) * 32 + lane] : 0u;
+#pragma unroll
+    for (int j = 0; j < CAP; j++) {
+      vt[j] = J[(e[j] >> (2 * B)) & M];
+      vm[j] = J[(e[j] >> B) & M];
+      vs[j] = J[e[j] & M];
     }
+    const int n_next = (it + 1 < K::IT_LU) ? lane_count(tab, K::O_CLU, it + 1, lane) : 0;
+#pragma unroll
+    for (int j = 0; j < CAP; j++)
+      if (j < n) J[(e[j] >> (2 * B)) & M] = (e[j] >> 31) ? vt[j] / vs[j] : vt[j] + (-vm[j]) * vs[j];
     pos += n;
+    n = n_next;
     __syncwarp();
   }
+  for (int i = lane; i < NVAR; i += 32) ry[i] = 1.0 / J[tab[K::O_DIAG + i]];
+  __syncwarp();
   return 0;
 }
 
-// Forward (BACKWARD = false) or backward substitution in place.
+// Forward (BACKWARD = false) or backward substitution in place; the backward
+// rows divide by U(i,i) through its reciprocal ry[i] (kpp_div_recip: the
+// same quotient as the division).
 template <bool BACKWARD>
-__device__ __forceinline__ void substitute(const unsigned* tab, const double* J, double* X,
-                                           int lane) {
-  constexpr int B = K::LU_BITS, C = K::X_BITS, F = B + 2 * C;
+__device__ __forceinline__ void substitute(const unsigned* __restrict__ tab, const double* J,
+                                           const double* ry, double* X, int lane) {
+  constexpr int B = K::LU_BITS, C = K::X_BITS, F = B + 2 * C, CAP = K::SOLVE_CAP;
   constexpr int OC = BACKWARD ? K::O_CBW : K::O_CFW;
   constexpr int OS = BACKWARD ? K::O_BW : K::O_FW;
   constexpr int IT = BACKWARD ? K::IT_BW : K::IT_FW;
   double acc = 0.0;
   int pos = 0;
+  int n = lane_count(tab, OC, 0, lane);
   for (int it = 0; it < IT; it++) {
-    const int n = lane_count(tab, OC, it, lane);
-    for (int j = 0; j < n; j++) {
-      const unsigned e = tab[OS + (pos + j) * 32 + lane];
-      const int a = e & ((1u << B) - 1), c = (e >> B) & ((1u << C) - 1);
-      const int r = (e >> (B + C)) & ((1u << C) - 1);
-      if ((e >> F) & 1u) acc = X[r];
-      if (!((e >> (F + 2)) & 1u)) acc = acc - J[a] * X[c];
-      if ((e >> (F + 1)) & 1u) X[r] = BACKWARD ? acc / J[tab[K::O_DIAG + r]] : acc;
+    unsigned e[CAP];
+    double jv[CAP], xv[CAP], xs[CAP], dv[CAP], yv[CAP];
+#pragma unroll
+    for (int j = 0; j < CAP; j++) e[j] = (j < n) ? tab[OS + (pos + j) * 32 + lane] : 0u;
+#pragma unroll
+    for (int j = 0; j < CAP; j++) {
+      const unsigned r = (e[j] >> (B + C)) & ((1u << C) - 1);
+      jv[j] = J[e[j] & ((1u << B) - 1)];
+      xv[j] = X[(e[j] >> B) & ((1u << C) - 1)];
+      xs[j] = X[r];
+      if (BACKWARD) {
+        dv[j] = J[tab[K::O_DIAG + r]];
+        yv[j] = ry[r];
+      }
+    }
+    const int n_next = (it + 1 < IT) ? lane_count(tab, OC, it + 1, lane) : 0;
+    // the running sums; a backward quotient comes from the reciprocal when
+    // its operands are in kpp_div_recip_ok's range, else from the division
+#pragma unroll
+    for (int j = 0; j < CAP; j++) {
+      if (j < n) {
+        if ((e[j] >> F) & 1u) acc = xs[j];
+        if (!((e[j] >> (F + 2)) & 1u)) acc = acc - jv[j] * xv[j];
+        if ((e[j] >> (F + 1)) & 1u)
+          X[(e[j] >> (B + C)) & ((1u << C) - 1)] =
+              BACKWARD ? kpp_div_recip(acc, dv[j], yv[j]) : acc;
+      }
     }
     pos += n;
+    n = n_next;
     __syncwarp();
   }
 }
 
 // Solve (LU) x = b in place, b given in X.
-__device__ __forceinline__ void solve(const unsigned* tab, const double* J, double* X, int lane) {
-  substitute<false>(tab, J, X, lane);
-  substitute<true>(tab, J, X, lane);
+__device__ __forceinline__ void solve(const unsigned* __restrict__ tab, const double* J,
+                                      const double* ry, double* X, int lane) {
+  substitute<false>(tab, J, ry, X, lane);
+  substitute<true>(tab, J, ry, X, lane);
 }
 
 // ---- vector operations of the integrator (util/blas.c), lane-strided -------
@@ -300,7 +370,7 @@ __device__ int integrate(const unsigned* tab, const double* kc, const Weights& w
         for (;;) {
           const double ghinv = 1.0 / (direction * h * tab_m.Gamma[0]);
           jac_matrix<S>(tab, kc, w.j, sm, ghinv, lane);
-          const int ising = decomp(tab, jvs, lane);
+          const int ising = decomp(tab, jvs, sm + L::RY, lane);
           st.ndec++;
           if (ising == 0) break;
           st.nsng++;
@@ -335,7 +405,7 @@ __device__ int integrate(const unsigned* tab, const double* kc, const Weights& w
           const double hg = direction * h * tab_m.Gamma[s];
           vaxpy(hg, dfdt, kst(s), lane);
         }
-        solve(tab, jvs, kst(s), lane);
+        solve(tab, jvs, sm + L::RY, kst(s), lane);
         st.nsol++;
       }
 

@@ -45,6 +45,14 @@
 #ifndef KPP_PART
 #define KPP_PART 0
 #endif
+// Default of the automatic kernel choice's cell limit (kpp_b200_set_auto_warp_cells).
+#ifndef KPP_COOP_MAX_CELLS
+#if defined(KPP_SCRATCH)
+#define KPP_COOP_MAX_CELLS 32768  // the crossing point measured for saprc99 on B200
+#else
+#define KPP_COOP_MAX_CELLS 0
+#endif
+#endif
 
 namespace kpp_b200_impl {
 #include "kpp_cell.cuh"
@@ -360,8 +368,9 @@ __device__ __forceinline__ void one_call(const LaunchArgs& a, W& w, const CellEn
 // lanes of a warp call this together (has = false: no cell, the lane only
 // joins the barriers), and a warp barrier after each call starts the lanes'
 // next chemistry step together, so the lanes stay in the same phase of the
-// integrator instead of drifting apart over the calls.
-template <int METHOD, bool CHAIN, class W>
+// integrator instead of drifting apart over the calls; with ALIGN = false
+// (lanes that take their cells one by one) there is no barrier.
+template <int METHOD, bool CHAIN, bool ALIGN = true, class W>
 __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, int cell,
                                                      bool has = true) {
   const long ld = a.ld;
@@ -377,7 +386,7 @@ __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, 
   if (CHAIN) {
     for (int k = 0; k < a.nchain; k++) {
       if (has) one_call<METHOD, true>(a, w, env, cell, k, t0, rpar2);
-      __syncwarp();
+      if (ALIGN) __syncwarp();
     }
   } else {
     one_call<METHOD, false>(a, w, env, cell, 0, t0, rpar2);
@@ -394,6 +403,9 @@ __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, 
 // (persistent launch: the grid is the resident thread count) and runs the
 // chained calls of each cell.  A queue ordered by decreasing cost hands the
 // long cells out first and keeps the 32 cells of a warp of similar cost.
+// With a.lane_queue each lane instead takes the next single position as soon
+// as its previous cell is done, so no lane waits for the slowest cell of its
+// warp (the lanes then run different cells' phases side by side).
 template <int METHOD, bool QUEUE>
 __global__ void
 #if KPP_MIN_BLOCKS > 0
@@ -404,7 +416,13 @@ __launch_bounds__(128)
 rosenbrock_kernel(const LaunchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   Work w(a.scratch, a.nslots, slot);
-  if (QUEUE) {
+  if (QUEUE && a.lane_queue) {
+    for (;;) {
+      const int pos = atomicAdd(a.queue, 1);
+      if (pos >= a.ncells) break;
+      integrate_cell_calls<METHOD, true, false>(a, w, a.order ? a.order[pos] : pos);
+    }
+  } else if (QUEUE) {
     const int lane = threadIdx.x & 31;
     for (;;) {
       int base = 0;
@@ -591,15 +609,21 @@ thread_local char g_last_error[512] = "";
 // (kpp_coop.cuh).  The warp-per-cell kernel runs only launches whose rate
 // constants are fixed for the call; the others always use the thread kernel.
 int g_kernel_choice = 0;
-// What the automatic choice picks for launches the warp-per-cell kernel supports.
-constexpr bool kCoopByDefault = false;
+// Work-queue granularity of the chained entry's thread-per-cell kernel: 0 a
+// warp takes 32 cells at a time, 1 each lane takes one cell at a time.
+std::atomic<int> g_lane_queue{0};
+// The automatic choice runs launches of at most this many cells on the
+// warp-per-cell kernel: the thread-per-cell kernel needs about 150k cells to
+// fill a B200 and is far slower below that, while the warp-per-cell kernel
+// fills it with 1776 cells (12 per SM) and then stays at its throughput.
+std::atomic<int> g_coop_max_cells{KPP_COOP_MAX_CELLS};
 
 bool use_coop(const LaunchArgs& a) {
 #if KPP_COOP
   if (!coop_supports(a)) return false;
   if (g_kernel_choice == 2) return true;
   if (g_kernel_choice == 1) return false;
-  return kCoopByDefault;
+  return a.ncells <= g_coop_max_cells.load();
 #else
   (void)a;
   return false;
@@ -730,14 +754,18 @@ long slots_for(int ncells) {
   if (cap > 0 && cap < per_sm) per_sm = cap;
   long res = (long)sms * per_sm * kBlock;
   long want = ((long)ncells + kBlock - 1) / kBlock * kBlock;
-  if (res > kSlotStride) res = kSlotStride;
   return want < res ? want : res;
 }
 
-// The scratch layout always spans kSlotStride slots (its stride is fixed).
-size_t scratch_bytes(long) {
-  return kUsesScratch ? (size_t)kScratchPerSlot * (size_t)kSlotStride * sizeof(double) : 0;
+// Work storage of `nslots` thread slots with `per_slot` doubles each, in the
+// warp-blocked scratch layout (whole warps).
+size_t slot_bytes(long per_slot, long nslots) {
+  return kUsesScratch ? (size_t)per_slot * (size_t)((nslots + kLanes - 1) / kLanes * kLanes) *
+                            sizeof(double)
+                      : 0;
 }
+
+size_t scratch_bytes(long nslots) { return slot_bytes(kScratchPerSlot, nslots); }
 
 // Library-managed work buffers, one per (device, stream), grown on demand and
 // kept until exit.  Growing calls cudaMalloc, which synchronises the device.
@@ -790,6 +818,7 @@ int cached_counter(cudaStream_t stream, int** out) {
 size_t scratch_capacity_doubles(const LaunchArgs& a) { return a.scratch_doubles; }
 
 int launch_rosenbrock(LaunchArgs& a, cudaStream_t s) {
+#if KPP_COOP
   if (use_coop(a)) {
     switch (a.ipar[3]) {
       case 1: return launch_method_coop<1>(a, s);
@@ -799,6 +828,7 @@ int launch_rosenbrock(LaunchArgs& a, cudaStream_t s) {
       default: return launch_method_coop<4>(a, s);
     }
   }
+#endif
   const int grid = (int)(a.nslots / kBlock);
   // Invalid methods are reported per cell by the validation in
   // rosenbrock_cell (IERR = -2); any valid instance does that.
@@ -842,6 +872,7 @@ int fill_args(LaunchArgs& a, int ncells, int ld, double* var, const double* fix,
   a.queue = nullptr;
   a.nchain = 0;
   a.chain_dt = 0.0;
+  a.lane_queue = 0;
   if (ipar) std::memcpy(a.ipar, ipar, sizeof a.ipar);
   if (rpar) std::memcpy(a.rpar, rpar, sizeof a.rpar);
   return KPP_B200_OK;
@@ -1016,8 +1047,7 @@ int host_pipeline(int ncells, int ld, double* var, const double* fix, const doub
       rc = launch_rosenbrock(a, s);
     } else {
       const long per = which == 1 ? kSdirkPerSlot : kRkPerSlot;
-      const size_t bytes =
-          kUsesScratch ? (size_t)per * (size_t)kSlotStride * sizeof(double) : 0;
+      const size_t bytes = slot_bytes(per, a.nslots);
       rc = cached_scratch(s, bytes, &a.scratch);
       if (rc != KPP_B200_OK) return rc;
       a.scratch_doubles = bytes / sizeof(double);
@@ -1184,8 +1214,7 @@ int kpp_b200_sdirk(int ncells, int ld, double* var, const double* fix, const dou
   if (rc != KPP_B200_OK || ncells == 0) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   a.nslots = slots_for(ncells);
-  const size_t bytes = kUsesScratch ? (size_t)kSdirkPerSlot * (size_t)kSlotStride * sizeof(double)
-                                    : 0;
+  const size_t bytes = slot_bytes(kSdirkPerSlot, a.nslots);
   rc = cached_scratch(s, bytes, &a.scratch);
   if (rc != KPP_B200_OK) return rc;
   a.scratch_doubles = bytes / sizeof(double);
@@ -1203,8 +1232,7 @@ int kpp_b200_runge_kutta(int ncells, int ld, double* var, const double* fix,
   if (rc != KPP_B200_OK || ncells == 0) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   a.nslots = slots_for(ncells);
-  const size_t bytes = kUsesScratch ? (size_t)kRkPerSlot * (size_t)kSlotStride * sizeof(double)
-                                    : 0;
+  const size_t bytes = slot_bytes(kRkPerSlot, a.nslots);
   rc = cached_scratch(s, bytes, &a.scratch);
   if (rc != KPP_B200_OK) return rc;
   a.scratch_doubles = bytes / sizeof(double);
@@ -1228,6 +1256,7 @@ int kpp_b200_rosenbrock_chain(int ncells, int ld, double* var, const double* fix
   a.nchain = ncalls;
   a.chain_dt = dt;
   a.order = order;
+  a.lane_queue = g_lane_queue.load();
   if (!use_coop(a)) {  // the warp-per-cell kernel needs no work buffer
     a.nslots = slots_for(ncells);
     rc = cached_scratch(s, scratch_bytes(a.nslots), &a.scratch);
@@ -1384,11 +1413,27 @@ int kpp_b200_set_kernel(int which) {
 
 int kpp_b200_get_kernel(void) {
 #if KPP_COOP
-  return g_kernel_choice == 2 || (g_kernel_choice == 0 && kCoopByDefault) ? 2 : 1;
+  return g_kernel_choice == 2 ? 2 : 1;
 #else
   return 1;
 #endif
 }
+
+int kpp_b200_set_queue_lanes(int per_lane) {
+  if (per_lane < 0 || per_lane > 1) return fail(KPP_B200_EINVAL, "queue granularity must be 0 or 1");
+  g_lane_queue.store(per_lane);
+  return KPP_B200_OK;
+}
+
+int kpp_b200_get_queue_lanes(void) { return g_lane_queue.load(); }
+
+int kpp_b200_set_auto_warp_cells(int ncells) {
+  if (ncells < 0) return fail(KPP_B200_EINVAL, "the cell limit must be >= 0");
+  g_coop_max_cells.store(ncells);
+  return KPP_B200_OK;
+}
+
+int kpp_b200_get_auto_warp_cells(void) { return g_coop_max_cells.load(); }
 
 int kpp_b200_set_blocks_per_sm(int blocks) {
   if (blocks < 0 || blocks > 64) return fail(KPP_B200_EINVAL, "blocks per SM must be 0..64");

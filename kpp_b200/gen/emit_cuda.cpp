@@ -685,7 +685,7 @@ void emit_coop_tables(std::ostream& o, const Mechanism& m) {
       jsum.push_back(t);
       jdiag.push_back(i == j);
     }
-  const int ncoef = (int)kc.size();
+  const int nsumcoef = (int)kc.size();  // codes of the sums' coefficients come first
   std::vector<unsigned> wa, wb;  // weight words: rct | k1 code | k2 code
   const int RB = bits_for(nr + 1);
   auto weights = [&](const std::vector<Prod>& ps, std::vector<unsigned>& out) {
@@ -695,8 +695,9 @@ void emit_coop_tables(std::ostream& o, const Mechanism& m) {
   };
   weights(pa, wa);
   weights(pb, wb);
+  const int ncoef = (int)kc.size();  // every constant, the weights' included
   const int B = bits_for(m.lu_nonzero), C = bits_for(nvar);
-  CoopSumLayout SL{bits_for(std::max<size_t>({pa.size(), pb.size(), 2})), bits_for(ncoef),
+  CoopSumLayout SL{bits_for(std::max<size_t>({pa.size(), pb.size(), 2})), bits_for(nsumcoef),
                    bits_for(std::max(m.lu_nonzero, nvar))};
   const bool fits = m.lu_nonzero <= 1024 && nvar <= 128 && next <= 255 && maxf <= 4 &&
                     (long)kc.size() <= 4096 && RB + 24 <= 32 &&
@@ -773,7 +774,9 @@ void emit_coop_tables(std::ostream& o, const Mechanism& m) {
     << sum_terms_v << " and " << sum_terms_j << " terms)\n"
     << "constexpr int IT_LU = " << lu.count.size() << ", IT_FW = " << fw.count.size()
     << ", IT_BW = " << bw.count.size() << ";  // iterations\n"
-    << "constexpr int LU_BITS = " << B << ", X_BITS = " << C << ";\n";
+    << "constexpr int LU_BITS = " << B << ", X_BITS = " << C << ";\n"
+    << "constexpr int LU_CAP = " << kCoopLuCap << ", SOLVE_CAP = " << kCoopSolveCap
+    << ";  // entries per lane per iteration\n";
   emit_table(o, "unsigned int", "tab", all);
   emit_dtable(o, "kc", kc);
   o << "}  // namespace kpp_coop\n";

@@ -1,13 +1,14 @@
 /* Hand-written scanner and parser for the KPP mechanism language.
  *
- * ORACLE INFRASTRUCTURE ONLY -- used by tests and the CPU baseline, never by
- * the product.  The reference KPP generator (the C sources in src/) is written against a
- * flex scanner (src/scan.l) and a bison parser (src/scan.y).  flex, bison and
- * libfl are not installed in this image, so the reference generator cannot be
- * built from its own Makefile (src/Makefile:38-54,86-93).  This file supplies
- * the symbols that lex.yy.c and y.tab.c would provide, so that the unchanged
- * reference sources in src/ (scanner.c, kpp.c, gen.c, code*.c, ...) link into
- * a working `kpp` binary that writes the reference's generated C code.
+ * KPP's generator (the C sources in src/) is written against a flex scanner
+ * (src/scan.l) and a bison parser (src/scan.y).  flex, bison and libfl are not
+ * installed in this image, so the generator cannot be built from its own
+ * Makefile (src/Makefile:38-54,86-93).  This file supplies the symbols that
+ * lex.yy.c and y.tab.c would provide, so that the unchanged sources in src/
+ * (scanner.c, kpp.c, gen.c, code*.c, ...) link into a working `kpp` binary.
+ * Two builds use it: the oracle's reference generator (oracle/build_ref.sh,
+ * the reference's own generated C code, for tests and the CPU baseline) and
+ * the generator with kpp_b200's CUDA target (kpp_b200/kppgen/build.py).
  *
  * Behaviour followed:
  *   - start conditions, patterns and actions of src/scan.l:37-298: flex

@@ -97,6 +97,8 @@ class Mechanism:
         L.kpp_b200_solve_tr.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
         L.kpp_b200_set_kernel.argtypes = [ctypes.c_int]
         L.kpp_b200_set_blocks_per_sm.argtypes = [ctypes.c_int]
+        L.kpp_b200_set_auto_warp_cells.argtypes = [ctypes.c_int]
+        L.kpp_b200_set_queue_lanes.argtypes = [ctypes.c_int]
         L.kpp_b200_sdirk.argtypes = ([ctypes.c_int, ctypes.c_int] + [_vp] * 9
                                      + [ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double)] + [_vp] * 4)
@@ -139,6 +141,22 @@ class Mechanism:
         """'auto', 'thread' (one thread per cell) or 'warp' (one warp per cell,
         work set in shared memory); both give bit-identical results."""
         self._check(self.lib.kpp_b200_set_kernel({"auto": 0, "thread": 1, "warp": 2}[which]))
+
+    def set_auto_warp_cells(self, ncells: int):
+        """Launches of at most `ncells` cells run on the warp-per-cell kernel
+        under the automatic choice (when it supports them); 0: never."""
+        self._check(self.lib.kpp_b200_set_auto_warp_cells(int(ncells)))
+
+    def auto_warp_cells(self) -> int:
+        return int(self.lib.kpp_b200_get_auto_warp_cells())
+
+    def set_queue_lanes(self, per_lane: bool):
+        """Work-queue granularity of rosenbrock_chain: each lane takes one
+        cell at a time (True) or each warp 32 (False, the default)."""
+        self._check(self.lib.kpp_b200_set_queue_lanes(1 if per_lane else 0))
+
+    def queue_lanes(self) -> bool:
+        return bool(self.lib.kpp_b200_get_queue_lanes())
 
     def user_species(self):
         """kpp_index[k] of every user species k (declaration order of the

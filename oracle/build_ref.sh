@@ -19,12 +19,13 @@
 #                                                 integrator (int/runge_kutta.c)
 #
 # The generator is compiled from the unchanged sources in $KPP_REF/src; only
-# the flex/bison front end is replaced by oracle/refkpp/frontend.c because
+# the flex/bison front end is replaced by kpp_b200/kppgen/frontend.c because
 # flex, bison and libfl are not installed.  Usage:
 #   oracle/build_ref.sh [KPP_REF=/path/to/reference] [mech ...]
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+FRONT="$HERE/../kpp_b200/kppgen"  # the hand-written scanner/parser of the KPP language
 KPP_REF="${KPP_REF:-/root/reference}"
 OUT="$HERE/_ref"
 MECHS=("$@")
@@ -43,10 +44,10 @@ echo "$KPP_REF" > "$OUT/kpp_home"
 # ---- 1. the generator -------------------------------------------------------
 GEN_SRCS=(code code_c code_f77 code_f90 code_matlab debug gen kpp scanner scanutil)
 for f in "${GEN_SRCS[@]}"; do
-  "$CC" -O -w -I"$HERE/refkpp" -I"$KPP_REF/src" -c "$KPP_REF/src/$f.c" -o "$OUT/obj/$f.o"
+  "$CC" -O -w -I"$FRONT" -I"$KPP_REF/src" -c "$KPP_REF/src/$f.c" -o "$OUT/obj/$f.o"
 done
-"$CC" -O -Wall -Wno-unused-function -I"$HERE/refkpp" -I"$KPP_REF/src" \
-  -c "$HERE/refkpp/frontend.c" -o "$OUT/obj/frontend.o"
+"$CC" -O -Wall -Wno-unused-function -I"$FRONT" -I"$KPP_REF/src" \
+  -c "$FRONT/frontend.c" -o "$OUT/obj/frontend.o"
 "$CC" "$OUT"/obj/*.o -lm -o "$OUT/kpp"
 
 # ---- 2. per-mechanism reference model ---------------------------------------
@@ -110,7 +111,7 @@ EOF
 
 # A mechanism whose outputs were built from the same oracle sources (this
 # script, refkpp/, ros_oracle.c, the MCM translator) is left as it is.
-SRC_KEY="$(cat "$HERE/build_ref.sh" "$HERE"/refkpp/*.c "$HERE"/refkpp/*.h "$HERE/ros_oracle.c" \
+SRC_KEY="$(cat "$HERE/build_ref.sh" "$HERE"/refkpp/*.c "$HERE"/refkpp/*.h "$FRONT/frontend.c" "$HERE/ros_oracle.c" \
   "$HERE"/../kpp_b200/gen/mcm.py "$HERE"/../kpp_b200/gen/fortran.py | sha256sum | cut -d' ' -f1)"
 
 for mech in "${MECHS[@]}"; do

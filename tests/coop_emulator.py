@@ -32,7 +32,8 @@ class CoopTables:
         self.c = {k: int(v) for k, v in re.findall(r"(\w+) = (-?\d+)", body)
                   if not k.startswith("__")}
         self.tab = self._array(body, "tab", int)
-        self.kc = self._array(body, "kc", float)
+        # the kernel stages NKC constants: an index beyond them must fail here too
+        self.kc = self._array(body, "kc", float)[: self.c["NKC"]]
         self.nvar = int(re.search(r"#define KPP_NVAR (\d+)", text).group(1))
         self.nfix = int(re.search(r"#define KPP_NFIX_TRUE (\d+)", text).group(1))
         self.lu_nz = int(re.search(r"#define KPP_LU_NONZERO (\d+)", text).group(1))
