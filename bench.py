@@ -55,11 +55,13 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "saprc99 cell-steps/s at 2^20 cells, learned-scheduled vs plain, same accuracy"
 UNIT = "cell-steps/s"
-# DRAM traffic of the thread-per-cell Rosenbrock kernel per internal step
-# (ncu: 212.0 GB over 1.62 M internal steps, 32768 fresh saprc99 cells,
-# profiles/rosenbrock_kernel_thread_saprc99_32k_fresh.md): the per-cell work
-# set (LU factors, stage vectors) streams through L2 to HBM.
-DRAM_BYTES_PER_INTERNAL_STEP = 212.0e9 / 1.619e6
+# DRAM traffic of the thread-per-cell Rosenbrock kernel per internal step at
+# full residency (ncu dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch over 2^17 fresh saprc99 cells, every thread slot of the GPU busy:
+# 990.0 + 311.4 GB over 6,480,123 internal steps,
+# profiles/rosenbrock_kernel_thread_saprc99_2p17_traffic.md): the per-cell
+# work set (LU factors, stage vectors) streams through L2 to HBM.
+DRAM_BYTES_PER_INTERNAL_STEP = (989962676736 + 311353660160) / 6480123
 # Compulsory bytes per cell-step: VAR in and out, FIX, TEMP, CFACTOR, SUN,
 # TSTART, TEND, Hstart in; ISTATUS, RSTATUS, IERR out (saprc99: 74 + 74 + 5 +
 # 6 doubles, 9 ints, 2 doubles).
@@ -192,11 +194,16 @@ class ClockSampler:
                     self.samples.append([x.strip() for x in out.split(",")])
             except Exception:
                 pass
+            self._first.set()
             self._stop.wait(0.2)
 
     def __enter__(self):
+        self._first = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        # the first query (thread start, process spawn) before the timed
+        # region opens, so that short steps do not carry it
+        self._first.wait(timeout=5.0)
         return self
 
     def __exit__(self, *exc):
@@ -691,8 +698,9 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                      "unit": "TFLOP/s", "frac": achieved_tflops / peak_fma if peak_fma > 0 else None,
                      "traffic": traffic_per_launch,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                                       "rosenbrock_kernel on 32768 fresh cells (profiles/), "
-                                       "per internal step, times this launch's internal steps",
+                                       "one rosenbrock_kernel launch over 2^17 fresh cells at "
+                                       "full residency (profiles/), per internal step, times "
+                                       "this launch's internal steps",
                      "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL_STEP * n,
                      "kernel_ms_per_launch": head.kernel_ms / args.steps,
                      "peak_source": "measured on this GPU by the DFMA throughput kernel "
@@ -1070,9 +1078,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--kernel", choices=["auto", "thread", "warp"], default="auto")
-    ap.add_argument("--queue", choices=["lanes", "warps"], default="lanes",
-                    help="work-queue granularity of the learned and ceiling arms: each lane "
-                         "takes one cell at a time, or each warp 32")
+    ap.add_argument("--queue", choices=["lanes", "warps"], default="warps",
+                    help="work-queue granularity of the learned and ceiling arms: each warp "
+                         "takes 32 cells at a time, or each lane one (measured equal)")
     ap.add_argument("--scheduler", choices=["learned", "plain"], default="learned")
     ap.add_argument("--weights", default=None, help="trained scheduler (.npz)")
     ap.add_argument("--accuracy-cells", type=int, default=4096,

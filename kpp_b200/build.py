@@ -4,6 +4,10 @@
   2. For each mechanism in kpp_b200/mechanisms/: kppcu writes the mechanism's
      CUDA device code (kpp_b200/_gen/<mech>.cuh), and nvcc builds the batched
      Rosenbrock library kpp_b200/lib/libkpp_b200_<mech>.so for sm_100a.
+  3. For the mechanisms of KPP_ROUTE, when KPP's sources are at hand: KPP's
+     own generator with kpp_b200's CUDA target (kpp_b200/kppgen) writes the
+     arithmetic, and the same kernels are built on it into
+     libkpp_b200_<mech>_kpproute.so.
 
 The kernel source is compiled once per part (the C ABI, and one part per
 Rosenbrock method) in parallel, then linked.  Builds are incremental: a
@@ -147,24 +151,31 @@ def generate(mech: str, kpp_home: str, force: bool = False) -> Path | None:
     return GEN_OUT / f"{mech}.cuh"
 
 
-def library_path(mech: str) -> Path:
-    return LIB / f"libkpp_b200_{mech}.so"
+def library_path(mech: str, route: str = "kppcu") -> Path:
+    """The mechanism library; route "kpp": built on the arithmetic that KPP's
+    own generator writes with #LANGUAGE CUDA (kpp_b200/kppgen)."""
+    return LIB / (f"libkpp_b200_{mech}.so" if route == "kppcu" else f"libkpp_b200_{mech}_kpproute.so")
 
 
-def compile_library(mech: str, header: Path, jobs: int, force: bool = False) -> Path:
+def compile_library(mech: str, header: Path, jobs: int, force: bool = False,
+                    route_dir: Path | None = None) -> Path:
     """nvcc each part (the C ABI, one part per Rosenbrock method, the SDIRK
     and the Runge-Kutta integrators) in parallel and link the shared library.  A part is recompiled only when its own
     preprocessed source or flags change (large mechanisms take many minutes
     per part), so a change confined to the C ABI rebuilds part 0 alone."""
     LIB.mkdir(exist_ok=True)
-    objdir = BUILD / mech
+    objdir = BUILD / (mech if route_dir is None else f"{mech}_kpproute")
     objdir.mkdir(parents=True, exist_ok=True)
     meta = json.loads((GEN_OUT / f"{mech}.json").read_text())
     defines = [f'-DKPP_MECH_HEADER="{header}"']
     if meta["lu_nonzero"] >= SCRATCH_LU_NONZERO:
         defines.append("-DKPP_SCRATCH")
+    if route_dir is not None:
+        defines += ["-DKPP_EXTERNAL_ARITHMETIC",
+                    f'-DKPP_ROUTE_INCLUDE="{route_dir / "route_includes.h"}"',
+                    "-I", str(route_dir), "-I", str(PKG / "kppgen"), "-I", str(CSRC)]
     host_header = GEN_OUT / f"{mech}_host.h"
-    lib = library_path(mech)
+    lib = library_path(mech, "kppcu" if route_dir is None else "kpp")
     parts = [0] + METHOD_PARTS + [SDIRK_PART, RK_PART]
 
     def part_flags(part: int):
@@ -242,6 +253,12 @@ def build_sched(force: bool = False) -> Path:
     return lib
 
 
+# Mechanisms whose library is also built on the KPP generator route (the
+# arithmetic written by KPP's own generator with #LANGUAGE CUDA), when KPP's
+# sources are at hand.
+KPP_ROUTE = ("small_strato", "saprc99")
+
+
 # Mechanisms built only when named (`python -m kpp_b200.build <mech>` or
 # `--all`), or once their library exists.  None at present: MCM isoprene's LU
 # and solve are loops over the LU tables (kppcu), so it builds with the rest.
@@ -257,7 +274,7 @@ def default_mechanisms():
 
 
 def build(mechs=None, force: bool = False, jobs: int | None = None, verbose: bool = True,
-          kpp_home: str | None = None):
+          kpp_home: str | None = None, route: bool = True):
     kpp_home = kpp_home if kpp_home is not None else default_kpp_home()
     jobs = jobs or os.cpu_count() or 4
     mechs = mechs or default_mechanisms()
@@ -274,6 +291,13 @@ def build(mechs=None, force: bool = False, jobs: int | None = None, verbose: boo
         built[mech] = compile_library(mech, header, jobs, force)
         if verbose:
             print(f"kpp_b200.build: {mech} -> {built[mech]}", flush=True)
+        if mech in KPP_ROUTE and route:
+            from .kppgen import build as kppgen
+            out = kppgen.generate(mech, kpp_home, force)
+            built[f"{mech}_kpproute"] = compile_library(mech, header, jobs, force, route_dir=out)
+            if verbose:
+                print(f"kpp_b200.build: {mech} (KPP generator route) -> "
+                      f"{built[f'{mech}_kpproute']}", flush=True)
     return built
 
 
@@ -285,9 +309,11 @@ def main(argv=None):
     ap.add_argument("--all", action="store_true", help="also the on-request mechanisms")
     ap.add_argument("--kpp-home", default=None,
                     help="KPP source tree with models/ and examples/ (default: $KPP_HOME)")
+    ap.add_argument("--no-kpp-route", dest="route", action="store_false",
+                    help="skip the libraries built on KPP's own generator (#LANGUAGE CUDA)")
     a = ap.parse_args(argv)
     build(a.mechs or (all_mechanisms() if a.all else None), force=a.force, jobs=a.jobs,
-          kpp_home=a.kpp_home)
+          kpp_home=a.kpp_home, route=a.route)
 
 
 if __name__ == "__main__":

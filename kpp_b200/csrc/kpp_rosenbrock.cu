@@ -32,6 +32,15 @@
 #include "../../include/kpp_b200.h"
 #include "kpp_ratelaws.cuh"
 #include KPP_MECH_HEADER
+#ifdef KPP_ROUTE_INCLUDE
+// The arithmetic written by KPP's own generator (#LANGUAGE CUDA,
+// kpp_b200/kppgen) in place of kppcu's; the warp-per-cell kernel, which runs
+// on kppcu's schedules, is left out of such a build.
+#include KPP_ROUTE_INCLUDE
+#include "route_adapter.cuh"
+#undef KPP_COOP
+#define KPP_COOP 0
+#endif
 #if KPP_PART == 7
 #include KPP_CMPLX_HEADER
 #endif

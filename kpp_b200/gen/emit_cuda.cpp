@@ -951,6 +951,10 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     << " on the time or the concentrations.\n"
     << "#define KPP_RATES_SUN " << ncls[RC_SUN] << "\n"
     << "#define KPP_RATES_DYNAMIC " << ncls[RC_DYNAMIC] << "\n\n";
+  // The arithmetic (rates, Fun, Jac_SP, LU, solve) can come from KPP's own
+  // generator instead (kpp_b200/kppgen: #LANGUAGE CUDA); such a build defines
+  // KPP_EXTERNAL_ARITHMETIC and supplies these functions itself.
+  o << "#ifndef KPP_EXTERNAL_ARITHMETIC\n";
   const char* names[3] = {"kpp_rconst_static", "kpp_rconst_sun", "kpp_rconst_dynamic"};
   for (int c = 0; c < 3; c++) {
     o << "template <class TR, class TV, class TF>\n"
@@ -1001,7 +1005,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     ops_fun += count_ops(sum);
     o << "  Vdot[" << i << "] = " << print(sum) << ";\n";
   }
-  o << "}\n\n";
+  o << "}\n#endif  // KPP_EXTERNAL_ARITHMETIC\n\n";
 
   // ---- Jac_SP
   std::vector<std::vector<int>> bidx(nr, std::vector<int>(nvar, -1));
@@ -1009,7 +1013,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
   for (int i = 0; i < nr; i++)
     for (int j = 0; j < nvar; j++)
       if (vw.left(j, i) != 0) bidx[i][j] = nb++;
-  o << "#define KPP_NJAC_TMP " << (nb > 0 ? nb : 1) << "\n\n";
+  o << "#define KPP_NJAC_TMP " << (nb > 0 ? nb : 1) << "\n\n#ifndef KPP_EXTERNAL_ARITHMETIC\n";
   o << "// Sparse Jacobian of one cell in the LU pattern (fill-in entries are 0);\n"
        "// NEG = true writes its negation (the -Jac0 of ros_PrepareMatrix).  B holds\n"
        "// the partial derivatives of the equation rates (KPP_NJAC_TMP entries).\n"
@@ -1051,7 +1055,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
        "__device__ __forceinline__ void kpp_add_diagonal(TJ& JVS, const double v) {\n";
   for (int i = 0; i < nvar; i++)
     o << "  JVS[" << m.lu_diag[i] << "] = JVS[" << m.lu_diag[i] << "] + v;\n";
-  o << "}\n\n";
+  o << "}\n#endif  // KPP_EXTERNAL_ARITHMETIC\n\n";
 
   // ---- KppDecomp and KppSolve.  Mechanisms below kGenericLu LU entries get
   // both fully unrolled; larger ones (MCM isoprene: 7123 entries, a 41k
@@ -1078,7 +1082,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
       }
     for (int i = 0; i < nvar; i++)
       ops_solve += 2L * (m.lu_crow[i + 1] - m.lu_crow[i] - 1) + 1;
-    o << "\n"
+    o << "\n#ifndef KPP_EXTERNAL_ARITHMETIC\n"
          "// In-place no-pivot sparse LU of one cell (KppDecomp, util/sutil.c:2-23), row by\n"
          "// row through the dense work row W of NVAR entries; returns k+1 when the\n"
          "// diagonal entry of row k is zero on entry to its elimination, 0 on success.\n"
@@ -1119,11 +1123,12 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
          "    for (int j = d + 1; j < kpp_lu_crow_c[i + 1]; j++) x = x - JVS[j]*X[kpp_lu_icol_c[j]];\n"
          "    X[i] = x/JVS[d];\n"
          "  }\n"
-         "}\n\n";
+         "}\n#endif  // KPP_EXTERNAL_ARITHMETIC\n\n";
   } else {
     std::vector<std::vector<int>> pos(nvar, std::vector<int>(nvar, -1));
     for (int k = 0; k < m.lu_nonzero; k++) pos[m.lu_irow[k]][m.lu_icol[k]] = k;
-    o << "// In-place no-pivot sparse LU of one cell (KppDecomp, util/sutil.c:2-23,\n"
+    o << "#ifndef KPP_EXTERNAL_ARITHMETIC\n"
+         "// In-place no-pivot sparse LU of one cell (KppDecomp, util/sutil.c:2-23,\n"
          "// unrolled in its operation order); returns k+1 when the diagonal entry of\n"
          "// row k is zero on entry to its elimination, 0 on success.  W (a work row\n"
          "// for the loop form of large mechanisms) is not used.\n"
@@ -1171,7 +1176,7 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
       ops_solve += count_ops(sum);
       o << "  X[" << i << "] = " << print(sum) << ";\n";
     }
-    o << "}\n\n";
+    o << "}\n#endif  // KPP_EXTERNAL_ARITHMETIC\n\n";
   }
 
   // ---- KppDecompCmplxR / KppSolveCmplxR (util/sutil.c:28-90), unrolled.

@@ -2,7 +2,7 @@
  * CUDA target of the KPP generator (#LANGUAGE CUDA).
  *
  * Part of kpp_b200: compiled into KPP's own generator together with its
- * unchanged sources (src/*.c of KPP 3.5.0) by kpp_b200/kppgen/build.py, which
+ * unchanged sources (the src directory of KPP 3.5.0) by kpp_b200/kppgen/build.py, which
  * adds this writer beside the C, Fortran and MATLAB ones and the hooks that
  * select it: a CUDA_LANG value of `enum lang` (src/gdata.h:93), the CUDA
  * argument of #LANGUAGE (CmdLanguage, src/scanner.c:284-308) and its case in
@@ -20,9 +20,9 @@
  *       template <class T0, ...> __device__ __forceinline__ void Fun(T0&& V, ...)
  *     so that a kernel passes thread-local arrays or strided views of
  *     per-cell work arrays in device memory;
- *   - Update_RCONST takes the generator's globals it reads as arguments
- *     (RCONST, TIME, TEMP, CFACTOR, SUN and the concentrations C), one cell
- *     per call;
+ *   - Update_RCONST and Update_PHOTO take the generator's globals they read
+ *     as arguments (RCONST, TIME, TEMP, CFACTOR, SUN and the concentrations
+ *     C), one cell per call;
  *   - the sparse-structure tables of <root>_JacobianSP.cu (LU_ICOL, ...) are
  *     device arrays (__device__ const), read by the LU of the util template;
  *   - the device-side files are <root>_Function.cu, _Jacobian.cu,
@@ -67,11 +67,12 @@ int narg, i;
   name = varTable[ f ]->name;
   narg = varTable[ f ]->maxi;
 
-  if( strcmp( name, "Update_RCONST" ) == 0 ) {
-    /* the globals the rate expressions and the C_RCONST code read */
+  if( narg == 0 && currentFile == rateFile ) {
+    /* Update_RCONST, Update_PHOTO: the globals the rate expressions and the
+       C_RCONST code read, as arguments */
     bprintf( "template <class TR, class TC>\n"
-             "__device__ __forceinline__ void Update_RCONST(\n"
-             "  TR&& RCONST,                           /* rate constants */\n"
+             "__device__ __forceinline__ void %s(\n", name );
+    bprintf( "  TR&& RCONST,                           /* rate constants */\n"
              "  const double TIME,                     /* model time */\n"
              "  const double TEMP,                     /* temperature */\n"
              "  const double CFACTOR,                  /* conversion factor */\n"
