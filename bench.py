@@ -285,25 +285,47 @@ def tight_reference(wl, cells, pool):
     return np.concatenate([r[0] for r in res], axis=1), np.concatenate([r[1] for r in res])
 
 
-def tight_gpu(mech, wl, cells, dev):
+def tight_gpu(mech, wl, cells, dev, ncalls: int = 1):
     """The same FP64 Rodas4 RTOL 1e-10 solution as tight_reference, for the
     given cells, by the library's own integrator (whose parity with the
-    reference the tests establish); returns (var, ierr, ms)."""
+    reference the tests establish); with ncalls > 1, over the driver loop of
+    ncalls chemistry steps (kpp_b200_rosenbrock_chain).  Returns (var, ierr,
+    ms)."""
     import torch
     from kpp_b200.controls import make_controls
     ipar, rpar = make_controls(method="rodas4", scalar_tol=True, max_steps=1_000_000)
     D = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     t0, t1 = wl.step_bounds(0)
     var = D(wl.var[:, cells])
+    args = dict(cfactor=None if wl.cfactor is None else D(wl.cfactor[cells]),
+                sun=None if wl.sun is None else D(wl.sun[cells]))
+    tol = (D(np.array([TIGHT_ATOL])), D(np.array([TIGHT_RTOL])))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    r = mech.rosenbrock(var, D(wl.fix[:, cells]), D(wl.temp[cells]), D(t0[cells]), D(t1[cells]),
-                        D(np.array([TIGHT_ATOL])), D(np.array([TIGHT_RTOL])), ipar, rpar,
-                        cfactor=None if wl.cfactor is None else D(wl.cfactor[cells]),
-                        sun=None if wl.sun is None else D(wl.sun[cells]))
+    if ncalls == 1:
+        r = mech.rosenbrock(var, D(wl.fix[:, cells]), D(wl.temp[cells]), D(t0[cells]),
+                            D(t1[cells]), *tol, ipar, rpar, **args)
+    else:
+        r = mech.rosenbrock_chain(var, D(wl.fix[:, cells]), D(wl.temp[cells]),
+                                  D(wl.tstart[cells]), wl.dt, ncalls, *tol, ipar, rpar, **args)
     e1.record()
     torch.cuda.synchronize()
     return var.cpu().numpy(), r.ierr.cpu().numpy(), e0.elapsed_time(e1)
+
+
+def accuracy_block(mech, wl, got, ncells, ncalls, dev, ncheck):
+    """accuracy() of a result `got` [NVAR, n] over `ncheck` cells evenly
+    spaced over the batch, against tight_gpu's solution of the same cells."""
+    cells = np.unique(np.linspace(0, ncells - 1, min(ncheck, ncells)).astype(np.int64))
+    ref, ref_ierr, tight_ms = tight_gpu(mech, wl, cells, dev, ncalls)
+    ok = ref_ierr == 1
+    out = accuracy(got[:, cells[ok]], ref[:, ok], float(wl.atol[0]), float(wl.rtol[0])) \
+        if ok.any() else None
+    return {"result": out,
+            "oracle": f"FP64 Rodas4, RTOL {TIGHT_RTOL:g}, ATOL {TIGHT_ATOL:g}, at most 10^6 "
+                      f"steps per call, {ncalls} chained call(s), on the GPU "
+                      f"({tight_ms / 1e3:.1f} s); cells evenly spaced over the batch",
+            "oracle_cells_ok": int(ok.sum()), "oracle_cells": int(ok.size)}
 
 
 def accuracy(got: np.ndarray, ref: np.ndarray, atol: float, rtol: float) -> dict:
@@ -462,6 +484,11 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                                              "nsol", "nsng"], map(int, self.ist)))}
 
     plain = Arm(False).run()
+    # the work queue alone: the plain controls (Hstart = STEPMIN) and cells in
+    # batch order, so its gain over plain is the queue's, none of it learned
+    queued = (Arm(False, fixed=(torch.zeros(n, dtype=torch.float64, device=dev),
+                                torch.arange(n, dtype=torch.int32, device=dev))).run()
+              if fresh and args.queue_arm else None)
     learned = Arm(True).run() if sched is not None else None
     head = learned if learned is not None else plain
     # the ceiling of a starting step plus cost order on this workload: every
@@ -615,6 +642,14 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         torch.cuda.synchronize()
         sched_block.update({
             "speedup_vs_plain": learned.value / plain.value,
+            "queue_cell_order": None if queued is None else {
+                "what": "kpp_b200_rosenbrock_chain, Hstart = STEPMIN, cells in batch order "
+                        f"({args.queue} queue): the work queue without the scheduler",
+                "value": queued.value, "speedup_vs_plain": queued.value / plain.value,
+                "bit_identical_to_plain": bool(np.array_equal(queued.var_out, plain.var_out)
+                                               and np.array_equal(queued.ierr, plain.ierr)),
+                "stats": queued.summary()},
+            "speedup_vs_queue_cell_order": None if queued is None else learned.value / queued.value,
             "plan_ms": e0.elapsed_time(e1) / 3,
             "ierr_identical_to_plain": bool(np.array_equal(learned.ierr, plain.ierr)),
             "ceiling": None if ceiling is None else dict(
@@ -730,7 +765,10 @@ def run_diurnal(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
-    wname = args.workload if args.workload.endswith("classes") else "saprc99_classes"
+    # saprc99: the uneven-stiffness classes; another mechanism: its own
+    # workload (small_strato: 72 x 1200 s steps of 4096 cells is config 1)
+    wname = (args.workload if args.workload.endswith("classes") or args.mech != "saprc99"
+             else "saprc99_classes")
     wl = workloads.for_mechanism(mech, wname, args.ncells, seed=shard_seed(rank))
     n, ncalls = wl.ncells, args.calls
     D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -777,7 +815,7 @@ def run_diurnal(args, rank, world, local_rank):
         REPO / "kpp_b200" / "schedulers" / "saprc99_uniform95.npz")
     var_c = var0.clone()
     box_c = [None]
-    if wpath.exists():
+    if wpath.exists() and args.mech == "saprc99":
         from kpp_b200.scheduler import LearnedScheduler
         sched = LearnedScheduler.load(wpath, mech.nvar)
         order = torch.empty(n, dtype=torch.int32, device=dev)
@@ -795,6 +833,10 @@ def run_diurnal(args, rank, world, local_rank):
 
         forms.append(("persistent_learned_order", persistent_learned))
 
+    # inputs smaller than L2 (126 MB): a 256 MB buffer written between the
+    # timed loops
+    small = wl.var.nbytes < (192 << 20)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if small else None
     results = {}
     for name, body in forms:
         with torch.cuda.stream(s):
@@ -808,14 +850,17 @@ def run_diurnal(args, rank, world, local_rank):
             for _ in range(args.warmup):
                 g.replay()
             torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
             with ClockSampler(local_rank) as clk:
-                e0.record(s)
-                for _ in range(args.steps):
+                for e0, e1 in evs:
+                    if flush is not None:
+                        flush.fill_(1)  # L2 flushed between timed loops, outside the events
+                    e0.record(s)
                     g.replay()
-                e1.record(s)
+                    e1.record(s)
                 torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
         if world > 1:
             ms = reduce_max(ms, dev)
         results[name] = {"ms_per_loop": ms / args.steps,
@@ -837,17 +882,26 @@ def run_diurnal(args, rank, world, local_rank):
                 classes[nm] = float(nstp[mask].mean() / ncalls)
     head = max(results.values(), key=lambda r: r["value"])
     head_name = [k for k, v in results.items() if v is head][0]
+    # the loop's final state against the tight solution of the whole loop
+    # (at most 1024 cells: each runs ncalls tight chemistry steps)
+    acc = (accuracy_block(mech, wl, var_b.cpu().numpy(), n, ncalls, dev,
+                          min(args.accuracy_cells, 1024)) if args.accuracy_cells > 0 else None)
     return {
-        "metric": f"{args.mech} cell-steps/s, {n} cells of uneven stiffness, {ncalls}-step "
-                  f"diurnal loop (persistent work queue vs one launch per step)",
+        "metric": f"{args.mech} cell-steps/s, {n} cells"
+                  + (" of uneven stiffness" if sza is not None else "")
+                  + f", {ncalls}-step diurnal loop (persistent work queue vs one launch per step)",
         "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_loop"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.mech} {wname}: 40 % day, 40 % night, 20 % within 5 deg "
-                               f"of the terminator; {ncalls} x {wl.dt:.0f} s Rodas3 steps, "
-                               f"RTOL 1e-3 ATOL 1e-2; one step = one diurnal loop of every cell",
+        "config": {"workload": f"{args.mech} {wname}: "
+                               + ("40 % day, 40 % night, 20 % within 5 deg of the terminator; "
+                                  if sza is not None else "start times over a whole day, SUN "
+                                  "from Update_SUN(TIME); ")
+                               + f"{ncalls} x {wl.dt:.0f} s Rodas3 steps, RTOL {wl.rtol[0]:g} "
+                                 f"ATOL {wl.atol[0]:g}; one step = one diurnal loop of every cell",
                    "cells_per_gpu": n, "graph": "both forms replayed from CUDA graphs",
-                   "l2": "inputs larger than L2"},
+                   "l2": ("inputs smaller than L2: 256 MB written between timed loops, "
+                          "outside the timed events" if small else "inputs larger than L2")},
         "impl": "kpp_b200", "gpu_launches": args.steps,
         "forms": results, "headline_form": head_name,
         "speedup_vs_per_step": {k: v["value"] / results["per_step"]["value"]
@@ -856,6 +910,7 @@ def run_diurnal(args, rank, world, local_rank):
         "internal_steps_per_cell_step": float(nstp.mean() / ncalls),
         "internal_steps_per_cell_step_by_class": classes,
         "ierr_ok_fraction": float((ob.ierr == 1).to(torch.float64).mean()),
+        "accuracy_vs_fp64_rtol1e-10": acc,
         "clocks": head["clocks"],
     }
 
@@ -958,6 +1013,8 @@ def run_integrator(args, rank, world, local_rank, kind: str):
     nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng = ist.tolist()
     ierr = box[0].ierr.cpu().numpy()
     var_dev = var.cpu().numpy()
+    acc = (accuracy_block(mech, wl, var_dev, n, 1, dev, args.accuracy_cells)
+           if args.accuracy_cells > 0 else None)
 
     # FP64 work from the counters.  SDIRK: Fun per Newton iteration, Jac +
     # LU per factorisation, a solve per Newton iteration and error estimate.
@@ -1047,6 +1104,7 @@ def run_integrator(args, rank, world, local_rank, kind: str):
                   "ierr_ok_fraction": float((ierr == 1).mean()),
                   "istatus_sum": dict(zip(["nfun", "njac", "nstp", "nacc", "nrej", "ndec",
                                            "nsol", "nsng"], map(int, ist)))},
+        "accuracy_vs_fp64_rtol1e-10": acc,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fma, "unit": "TFLOP/s",
                      "frac": achieved / peak_fma if peak_fma > 0 else None, "traffic": None,
                      "kernel_ms_per_launch": kernel_ms / args.steps,
@@ -1087,6 +1145,8 @@ def main():
                     help="cells compared with the FP64 RTOL 1e-10 solution (on the GPU)")
     ap.add_argument("--accuracy-cpu-cells", type=int, default=64,
                     help="of those, cells also solved by the CPU oracle as a cross-check")
+    ap.add_argument("--no-queue-arm", dest="queue_arm", action="store_false",
+                    help="skip the work-queue arm in cell order with the plain controls")
     ap.add_argument("--no-ceiling", dest="ceiling", action="store_false",
                     help="skip the ceiling arm (best starting step, true cost order)")
     args = ap.parse_args()

@@ -432,7 +432,8 @@ __device__ int integrate(const unsigned* tab, const double* kc, const Weights& w
       err = sqrt(err / (double)NVAR);
       __syncwarp();
 
-      const double fac = ros_min(facmax, ros_max(facmin, facsafe / pow(err, 1.0 / tab_m.ELO)));
+      const double fac =
+          ros_min(facmax, ros_max(facmin, facsafe / KPP_POW(err, 1.0 / tab_m.ELO)));
       double hnew = h * fac;
 
       st.nstp++;

@@ -168,3 +168,131 @@ __device__ __forceinline__ double kpp_update_sun(double TIME) {
   }
   return 0.0;
 }
+
+// ---------------------------------------------------------------------------
+// kpp_pow_cr(x, y): x^y correctly rounded to nearest (to within a final
+// double-double error of about 2^-98 relative, so misrounded only for
+// arguments whose exact result lies that close to a rounding midpoint).  It
+// is the pow() of the integrators' step-size and Newton controllers
+// (KPP_POW), whose results decide whether a step is accepted, a Jacobian
+// reused or a Newton iteration stopped: with a correctly rounded pow those
+// decisions follow the reference's wherever the C library's pow (which the
+// reference calls) is correctly rounded.  Method, in double-double
+// arithmetic (the operations above):
+//   * x = 2^e m with m in [1/sqrt(2), sqrt(2)) (frexp);
+//   * log m = 2 atanh(s), s = (m - 1)/(m + 1), |s| <= 0.1716, by the series
+//     sum s^(2n+1)/(2n+1) (terms n <= 10 in double-double, n = 11..21 in
+//     double, where they are below 2^-53 of the sum);
+//   * log x = e ln2 + log m with ln2 split in three parts (Cody and Waite's
+//     reduction: the first has 42 bits, so e * part exactly for |e| < 2^11);
+//   * t = y log x; exp t = 2^k exp(r), k = nearest integer to t / ln2,
+//     r = t - k ln2 by the same three-part split; exp(r) = (1 + u)^16 with
+//     u = expm1(r / 16) by its Taylor series (terms n <= 7 in double-double,
+//     the rest in double) and four squarings in the form u <- 2u + u^2;
+//   * the double-double result rounded once to double, then scaled by 2^k.
+// Special arguments (x or y zero, infinite or NaN; x negative with y not an
+// integer) and results outside the normal range (|t| > 708) return the C
+// library's pow(x, y): their values are exact (0, 1, inf, NaN) or, for the
+// extremes, never reached by the controllers.  y = 1, 2, -1 and 1/2 are x,
+// x*x, 1/x and sqrt(x), one correctly rounded operation each (which also
+// settles their exact midpoint cases).  Constants: ln2 in three
+// parts, 1/(2n+1) and 1/(n+1)! rounded to double-double.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ kpp_dd kpp_dd_mul_d(kpp_dd x, double y) {
+  double p = x.hi * y;
+  double e = kpp_fma(x.hi, y, -p);
+  e += x.lo * y;
+  return kpp_fast_two_sum(p, e);
+}
+
+__host__ __device__ __forceinline__ kpp_dd kpp_two_prod(double a, double b) {
+  double p = a * b;
+  return {p, kpp_fma(a, b, -p)};
+}
+
+__host__ __device__ inline double kpp_pow_cr(double x, double y) {
+  if (y == 0.0 || x == 1.0) return 1.0;
+  if (x != x || y != y) return x + y;
+  const double ax = fabs(x);
+  bool negate = false;
+  if (x < 0.0) {
+    if (y != trunc(y)) return pow(x, y);  // NaN
+    negate = fabs(y) < 9007199254740992.0 && fmod(y, 2.0) != 0.0;
+  }
+  if (ax == 0.0 || isinf(ax) || isinf(y)) return pow(x, y);
+  // exponents whose power is one IEEE operation, correctly rounded by itself
+  if (y == 1.0) return x;
+  if (y == 2.0) return x * x;
+  if (y == -1.0) return 1.0 / x;
+  if (y == 0.5) return sqrt(x);  // x > 0 here
+
+  const double L1 = 0.6931471805598903, L2 = 5.497923018708371e-14, L3 = 1.94704509238075e-31;
+  const double at[11][2] = {
+      {1.0, 0.0}, {0.3333333333333333, 1.850371707708594e-17}, {0.2, -1.1102230246251566e-17},
+      {0.14285714285714285, 7.93016446160826e-18}, {0.1111111111111111, 6.1679056923619804e-18},
+      {0.09090909090909091, -2.523234146875356e-18}, {0.07692307692307693, -4.270088556250602e-18},
+      {0.06666666666666667, 9.251858538542971e-19}, {0.058823529411764705, 8.163404592832033e-19},
+      {0.05263157894736842, 2.921639538487254e-18}, {0.047619047619047616, 2.64338815386942e-18}};
+  const double ex[8][2] = {
+      {1.0, 0.0}, {0.5, 0.0}, {0.16666666666666666, 9.25185853854297e-18},
+      {0.041666666666666664, 2.3129646346357427e-18}, {0.008333333333333333, 1.1564823173178714e-19},
+      {0.001388888888888889, -5.300543954373577e-20}, {0.0001984126984126984, 1.7209558293420705e-22},
+      {2.48015873015873e-05, 2.1511947866775882e-23}};
+
+  // log x
+  int e;
+  double m = frexp(ax, &e);
+  if (m < 0.7071067811865476) {
+    m *= 2.0;
+    e -= 1;
+  }
+  const double num = m - 1.0;  // exact: m in [0.5, 2]
+  const kpp_dd den = kpp_two_sum(m, 1.0);
+  kpp_dd s;
+  {
+    double q1 = num / den.hi;
+    kpp_dd r = kpp_dd_add({num, 0.0}, kpp_dd_mul_d(den, -q1));
+    double q2 = r.hi / den.hi;
+    r = kpp_dd_add(r, kpp_dd_mul_d(den, -q2));
+    double q3 = r.hi / den.hi;
+    s = kpp_dd_add(kpp_fast_two_sum(q1, q2), {q3, 0.0});
+  }
+  const kpp_dd s2 = kpp_dd_mul(s, s);
+  double tail = 1.0 / 43.0;
+  for (int n = 20; n >= 11; n--) tail = tail * s2.hi + 1.0 / (double)(2 * n + 1);
+  kpp_dd p = kpp_dd_add(kpp_dd_mul_d(s2, tail), {at[10][0], at[10][1]});
+  for (int n = 9; n >= 0; n--) p = kpp_dd_add(kpp_dd_mul(p, s2), {at[n][0], at[n][1]});
+  kpp_dd lm = kpp_dd_mul(s, p);
+  lm.hi *= 2.0;
+  lm.lo *= 2.0;
+  const double de = (double)e;
+  kpp_dd lx = kpp_dd_add(kpp_two_prod(de, L2), {de * L3, 0.0});
+  lx = kpp_dd_add(kpp_dd_add({de * L1, 0.0}, lx), lm);
+
+  // t = y log x, exp t
+  const kpp_dd t = kpp_dd_mul_d(lx, y);
+  if (!(fabs(t.hi) <= 708.0)) return pow(x, y);
+  const double kf = rint(t.hi * 1.4426950408889634);
+  kpp_dd r = kpp_two_sum(t.hi - kf * L1, t.lo);  // t.hi - kf*L1 is exact
+  r = kpp_dd_add(r, kpp_two_prod(-kf, L2));
+  r = kpp_dd_add(r, {-kf * L3, 0.0});
+  r.hi *= 0.0625;
+  r.lo *= 0.0625;
+  double et = 1.1470745597729725e-11;
+  const double tcoef[5] = {2.7557319223985893e-06, 2.755731922398589e-07, 2.505210838544172e-08,
+                           2.08767569878681e-09, 1.6059043836821613e-10};
+  for (int n = 4; n >= 0; n--) et = et * r.hi + tcoef[n];
+  kpp_dd q = kpp_dd_add(kpp_dd_mul_d(r, et), {ex[7][0], ex[7][1]});
+  for (int n = 6; n >= 0; n--) q = kpp_dd_add(kpp_dd_mul(q, r), {ex[n][0], ex[n][1]});
+  kpp_dd u = kpp_dd_mul(r, q);
+  for (int i = 0; i < 4; i++) u = kpp_dd_add({2.0 * u.hi, 2.0 * u.lo}, kpp_dd_mul(u, u));
+  const kpp_dd E = kpp_dd_add({1.0, 0.0}, u);
+  const double v = ldexp(E.hi, (int)kf);
+  return negate ? -v : v;
+}
+
+// The pow of the integrators' controllers (the host harness of the tests
+// substitutes the C library's to compare with the reference bit for bit).
+#ifndef KPP_POW
+#define KPP_POW kpp_pow_cr
+#endif

@@ -605,10 +605,10 @@ __device__ __forceinline__ bool sdirk_newton(const CellEnv& env, const Controls&
       if (theta_sd < 0.99) {
         rate = theta_sd / (1.0 - theta_sd);
         const double predicted =
-            inc * pow(theta_sd, (double)(c.newton_maxit - it)) / (1.0 - theta_sd);
+            inc * KPP_POW(theta_sd, (double)(c.newton_maxit - it)) / (1.0 - theta_sd);
         if (predicted >= c.newton_tol) {
           const double qn = ros_min(10.0, predicted / c.newton_tol);
-          fac = 0.8 * pow(qn, (-1.0 / (double)(1 + c.newton_maxit - it)));
+          fac = 0.8 * KPP_POW(qn, (-1.0 / (double)(1 + c.newton_maxit - it)));
           break;
         }
       } else {
@@ -693,10 +693,10 @@ __device__ int integrate(const CellEnv& env, W& w, const Controls& c, double t, 
         }
         if (it < c.newton_maxit) {
           const double predicted =
-              inc * pow(theta, (double)(c.newton_maxit - it)) / (1.0 - theta);
+              inc * KPP_POW(theta, (double)(c.newton_maxit - it)) / (1.0 - theta);
           if (predicted >= c.newton_tol) {
             const double qn = ros_min(10.0, predicted / c.newton_tol);
-            fac = 0.8 * pow(qn, (-1.0 / (double)(1 + c.newton_maxit - it)));
+            fac = 0.8 * KPP_POW(qn, (-1.0 / (double)(1 + c.newton_maxit - it)));
             break;
           }
         }
@@ -749,7 +749,7 @@ __device__ int integrate(const CellEnv& env, W& w, const Controls& c, double t, 
     }
 
     // new step size (the main loop's Newton count)
-    fac = pow(err, (-1.0 / m.elo)) *
+    fac = KPP_POW(err, (-1.0 / m.elo)) *
           ros_min(c.facsafe,
                   (1.0 + 2 * c.newton_maxit) / (double)(it_main + 2 * c.newton_maxit));
     fac = ros_min(c.facmax, ros_max(c.facmin, fac));
@@ -759,7 +759,7 @@ __device__ int integrate(const CellEnv& env, W& w, const Controls& c, double t, 
       st.nacc++;
       if (c.gustafsson) {
         if (st.nacc > 1) {
-          double facgus = c.facsafe * (h / hacc) * pow(err * err / errold, -0.25);
+          double facgus = c.facsafe * (h / hacc) * KPP_POW(err * err / errold, -0.25);
           facgus = ros_min(c.facmax, ros_max(c.facmin, facgus));
           fac = ros_min(fac, facgus);
           hnew = fac * h;

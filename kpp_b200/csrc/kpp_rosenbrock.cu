@@ -106,165 +106,228 @@ __device__ __forceinline__ bool prepare_matrix(const CellEnv& env, double t, dou
   }
 }
 
-// RosenbrockIntegrator (int/rosenbrock.c:450-627) for one cell; w.y holds
-// the cell state in and out.
+// Controls of one Rosenbrock call after validation and defaults.
+struct RosControls {
+  bool autonomous, vectortol;
+  int max_no_steps;
+  double hmin, hmax, hstart, facmin, facmax, facrej, facsafe;
+  const double *atol, *rtol;
+};
+
+// Rosenbrock (int/rosenbrock.c:137-446): validation and defaults of a call
+// over [tstart, tend] whose Hstart is rpar2 (RPAR[2], or the cell's own).
+// Returns 0, or the IERR (-1..-5) of the first rejected control in the
+// reference's order of checks.
+__device__ __forceinline__ int ros_controls(const LaunchArgs& a, double tstart, double tend,
+                                            double rpar2, RosControls& c) {
+  const int* ipar = a.ipar;
+  const double* rpar = a.rpar;
+  c.atol = a.atol;
+  c.rtol = a.rtol;
+  c.autonomous = !(ipar[0] == 0);
+  c.vectortol = (ipar[1] == 0);
+  const int uplimtol = c.vectortol ? NVAR : 1;
+  c.max_no_steps = (ipar[2] == 0) ? 100000 : ipar[2];
+  if (c.max_no_steps < 0) return KPP_B200_IERR_MAXSTEPS_BAD;
+  if ((ipar[3] < 1) || (ipar[3] > 5)) return KPP_B200_IERR_METHOD;
+  c.hmin = rpar[0];
+  if (rpar[0] < 0.0) return KPP_B200_IERR_HBOUNDS;
+  c.hmax = (rpar[1] == 0.0) ? ros_abs_diff(tend, tstart)
+                            : ros_min(ros_abs(rpar[1]), ros_abs_diff(tend, tstart));
+  if (rpar[1] < 0.0) return KPP_B200_IERR_HBOUNDS;
+  c.hstart = (rpar2 == 0.0) ? ros_max(c.hmin, kDeltaMin)
+                            : ros_min(ros_abs(rpar2), ros_abs_diff(tend, tstart));
+  if (rpar2 < 0.0) return KPP_B200_IERR_HBOUNDS;
+  c.facmin = (rpar[3] == 0.0) ? 0.2 : rpar[3];
+  if (rpar[3] < 0.0) return KPP_B200_IERR_FACTORS;
+  c.facmax = (rpar[4] == 0.0) ? 6.0 : rpar[4];
+  if (rpar[4] < 0.0) return KPP_B200_IERR_FACTORS;
+  c.facrej = (rpar[5] == 0.0) ? 0.1 : rpar[5];
+  if (rpar[5] < 0.0) return KPP_B200_IERR_FACTORS;
+  c.facsafe = (rpar[6] == 0.0) ? 0.9 : rpar[6];
+  if (rpar[6] < 0.0) return KPP_B200_IERR_FACTORS;
+  for (int i = 0; i < uplimtol; i++)
+    if ((c.atol[i] <= 0.0) || (c.rtol[i] <= 10.0 * kRoundoff) || (c.rtol[i] >= 1.0))
+      return KPP_B200_IERR_TOLERANCES;
+  return 0;
+}
+
+// RosenbrockIntegrator's state (int/rosenbrock.c:450-627) between its steps.
+struct RosState {
+  double t, tend, h, hexit;
+  int direction;
+  bool reject_last, reject_more, varying;
+};
+
+// Start of RosenbrockIntegrator (:450-470); w.y holds the cell state.
+template <class W>
+__device__ __forceinline__ void ros_begin(const CellEnv& env, W& w, const RosControls& c,
+                                          double tstart, double tend, RosState& s) {
+  s.t = tstart;
+  s.tend = tend;
+  s.hexit = 0.0;
+  s.h = ros_min(c.hstart, c.hmax);
+  if (ros_abs(s.h) <= 10.0 * kRoundoff) s.h = kDeltaMin;
+  s.direction = (tend >= tstart) ? +1 : -1;
+  s.reject_last = false;
+  s.reject_more = false;
+  s.varying = rates_vary<W>(env);
+  rates_once(env, s.t, w);
+}
+
+// Head of the time loop (:471-529): KPP_B200_IERR_SUCCESS when the loop is
+// done, -6 / -7 when the call fails, else 0 after Fcn0 = Fun(T, Y), dF/dT
+// and the Jacobian count (each attempt's prepare_matrix evaluates the
+// Jacobian itself).
+template <class W>
+__device__ __forceinline__ int ros_step_head(const CellEnv& env, W& w, const RosControls& c,
+                                             RosState& s, Stats& st) {
+  if (!(((s.direction > 0) && ((s.t - s.tend) + kRoundoff <= 0.0)) ||
+        ((s.direction < 0) && ((s.tend - s.t) + kRoundoff <= 0.0))))
+    return KPP_B200_IERR_SUCCESS;
+  if (st.nstp > c.max_no_steps) return KPP_B200_IERR_TOO_MANY_STEPS;
+  if (((s.t + 0.1 * s.h) == s.t) || (s.h <= kRoundoff)) return KPP_B200_IERR_STEP_TOO_SMALL;
+  s.hexit = s.h;
+  s.h = ros_min(s.h, ros_abs_diff(s.tend, s.t));
+
+  // FunTemplate(T, Y, Fcn0)
+  rates_at(env, s.t, w);
+  kpp_fun(w.y, env.fix, w.rconst, w.fcn0, w.a);
+  st.nfun++;
+  if (!c.autonomous) {
+    // ros_FunTimeDerivative (:663-682): dFdT = (Fun(T+Delta) - Fcn0)/Delta
+    double delta = sqrt(kRoundoff) * ros_max(kDeltaMin, ros_abs(s.t));
+    if (s.varying) {
+      rates_at(env, s.t + delta, w);
+      kpp_fun(w.y, env.fix, w.rconst, w.dfdt, w.a);
+      rates_at(env, s.t, w);  // JacTemplate(T) below sees the rates at T
+    } else {
+      // Fun(T+Delta) would see the same rates and state: Fcn0 again
+      copy(w.fcn0, w.dfdt);
+    }
+    st.nfun++;
+    axpy(-1.0, w.fcn0, w.dfdt);
+    double inv = 1.0 / delta;
+    if (inv != 1.0) {
+#pragma unroll 4
+      for (int i = 0; i < NVAR; i++) w.dfdt[i] = inv * w.dfdt[i];
+    }
+  }
+  st.njac++;  // JacTemplate(T, Y, Jac0), evaluated inside prepare_matrix
+  return 0;
+}
+
+// One attempt of the UntilAccepted loop (:531-611): 1 when the step is
+// accepted (T and Y advanced), 0 when it is rejected (H reduced: the next
+// attempt follows), or KPP_B200_IERR_SINGULAR.  `retry` is false for the
+// first attempt of a step.
 template <int METHOD, class W>
-__device__ int integrate_cell(const CellEnv& env, W& w, double tstart, double tend,
-                              const double* atol, const double* rtol, bool autonomous,
-                              bool vectortol, int max_no_steps, double hmin, double hmax,
-                              double hstart, double facmin, double facmax, double facrej,
-                              double facsafe, double& texit, double& hexit, Stats& st) {
+__device__ __forceinline__ int ros_attempt(const CellEnv& env, W& w, const RosControls& c,
+                                           RosState& s, bool& retry, Stats& st) {
   constexpr Tableau tab = make_tableau(METHOD);
   constexpr int S = tab.S;
-
-  double t = tstart;
-  hexit = 0.0;
-  double h = ros_min(hstart, hmax);
-  if (ros_abs(h) <= 10.0 * kRoundoff) h = kDeltaMin;
-  const int direction = (tend >= tstart) ? +1 : -1;
-  bool reject_last = false, reject_more = false;
-  const bool varying = rates_vary<W>(env);
-  rates_once(env, t, w);
-
-  while (((direction > 0) && ((t - tend) + kRoundoff <= 0.0)) ||
-         ((direction < 0) && ((tend - t) + kRoundoff <= 0.0))) {
-    if (st.nstp > max_no_steps) { texit = t; return KPP_B200_IERR_TOO_MANY_STEPS; }
-    if (((t + 0.1 * h) == t) || (h <= kRoundoff)) { texit = t; return KPP_B200_IERR_STEP_TOO_SMALL; }
-    hexit = h;
-    h = ros_min(h, ros_abs_diff(tend, t));
-
-    // FunTemplate(T, Y, Fcn0)
-    rates_at(env, t, w);
-    kpp_fun(w.y, env.fix, w.rconst, w.fcn0, w.a);
-    st.nfun++;
-    if (!autonomous) {
-      // ros_FunTimeDerivative (:663-682): dFdT = (Fun(T+Delta) - Fcn0)/Delta
-      double delta = sqrt(kRoundoff) * ros_max(kDeltaMin, ros_abs(t));
-      if (varying) {
-        rates_at(env, t + delta, w);
-        kpp_fun(w.y, env.fix, w.rconst, w.dfdt, w.a);
-        rates_at(env, t, w);  // JacTemplate(T) below sees the rates at T
-      } else {
-        // Fun(T+Delta) would see the same rates and state: Fcn0 again
-        copy(w.fcn0, w.dfdt);
-      }
-      st.nfun++;
-      axpy(-1.0, w.fcn0, w.dfdt);
-      double inv = 1.0 / delta;
-      if (inv != 1.0) {
-#pragma unroll 4
-        for (int i = 0; i < NVAR; i++) w.dfdt[i] = inv * w.dfdt[i];
-      }
-    }
-    st.njac++;  // JacTemplate(T, Y, Jac0), evaluated inside prepare_matrix
-
-    bool retry = false;
-    for (;;) {  // until the step is accepted
-      if (retry && varying) rates_at(env, t, w);  // stages moved the rates to Tau
-      retry = true;
-      if (prepare_matrix(env, t, h, direction, tab.Gamma[0], w, st)) {
-        texit = t;
-        return KPP_B200_IERR_SINGULAR;
-      }
+  const int direction = s.direction;
+  if (retry && s.varying) rates_at(env, s.t, w);  // stages moved the rates to Tau
+  retry = true;
+  if (prepare_matrix(env, s.t, s.h, direction, tab.Gamma[0], w, st))
+    return KPP_B200_IERR_SINGULAR;
+  const double h = s.h;
 #pragma unroll
-      for (int s = 0; s < S; s++) {
-        if (s == 0) {
-          copy(w.fcn0, w.fcn);
-        } else if (tab.NewF[s]) {
-          copy(w.y, w.ynew);
-#pragma unroll
-          for (int j = 0; j < s; j++) axpy(tab.A[s * (s - 1) / 2 + j], w.k[j], w.ynew);
-          double tau = t + tab.Alpha[s] * direction * h;
-          if (varying) rates_at(env, tau, w);
-          kpp_fun(w.ynew, env.fix, w.rconst, w.fcn, w.a);
-          st.nfun++;
-        }
-        copy(w.fcn, w.k[s]);
-#pragma unroll
-        for (int j = 0; j < s; j++) {
-          double hc = tab.C[s * (s - 1) / 2 + j] / (direction * h);
-          axpy(hc, w.k[j], w.k[s]);
-        }
-        if ((!autonomous) && (tab.Gamma[s] != 0.0)) {
-          double hg = direction * h * tab.Gamma[s];
-          axpy(hg, w.dfdt, w.k[s]);
-        }
-        kpp_solve(w.jvs, w.k[s]);
-        st.nsol++;
-      }
-
+  for (int j = 0; j < S; j++) {
+    if (j == 0) {
+      copy(w.fcn0, w.fcn);
+    } else if (tab.NewF[j]) {
       copy(w.y, w.ynew);
 #pragma unroll
-      for (int j = 0; j < S; j++) axpy(tab.M[j], w.k[j], w.ynew);
-#pragma unroll 4
-      for (int i = 0; i < NVAR; i++) w.yerr[i] = 0.0;
+      for (int i = 0; i < j; i++) axpy(tab.A[j * (j - 1) / 2 + i], w.k[i], w.ynew);
+      double tau = s.t + tab.Alpha[j] * direction * h;
+      if (s.varying) rates_at(env, tau, w);
+      kpp_fun(w.ynew, env.fix, w.rconst, w.fcn, w.a);
+      st.nfun++;
+    }
+    copy(w.fcn, w.k[j]);
 #pragma unroll
-      for (int j = 0; j < S; j++) axpy(tab.E[j], w.k[j], w.yerr);
-      double err = error_norm(w.y, w.ynew, w.yerr, atol, rtol, vectortol);
+    for (int i = 0; i < j; i++) {
+      double hc = tab.C[j * (j - 1) / 2 + i] / (direction * h);
+      axpy(hc, w.k[i], w.k[j]);
+    }
+    if ((!c.autonomous) && (tab.Gamma[j] != 0.0)) {
+      double hg = direction * h * tab.Gamma[j];
+      axpy(hg, w.dfdt, w.k[j]);
+    }
+    kpp_solve(w.jvs, w.k[j]);
+    st.nsol++;
+  }
 
-      double fac = ros_min(facmax, ros_max(facmin, facsafe / pow(err, 1.0 / tab.ELO)));
-      double hnew = h * fac;
+  copy(w.y, w.ynew);
+#pragma unroll
+  for (int j = 0; j < S; j++) axpy(tab.M[j], w.k[j], w.ynew);
+#pragma unroll 4
+  for (int i = 0; i < NVAR; i++) w.yerr[i] = 0.0;
+#pragma unroll
+  for (int j = 0; j < S; j++) axpy(tab.E[j], w.k[j], w.yerr);
+  double err = error_norm(w.y, w.ynew, w.yerr, c.atol, c.rtol, c.vectortol);
 
-      st.nstp++;
-      if ((err <= 1.0) || (h <= hmin)) {
-        st.nacc++;
-        copy(w.ynew, w.y);
-        t += direction * h;
-        hnew = ros_max(hmin, ros_min(hnew, hmax));
-        if (reject_last) hnew = ros_min(hnew, h);
-        reject_last = false;
-        reject_more = false;
-        h = hnew;
-        break;
-      } else {
-        if (st.nacc >= 1) st.nrej++;
-        if (reject_more) hnew = h * facrej;
-        reject_more = reject_last;
-        reject_last = true;
-        h = hnew;
+  double fac = ros_min(c.facmax, ros_max(c.facmin, c.facsafe / KPP_POW(err, 1.0 / tab.ELO)));
+  double hnew = h * fac;
+
+  st.nstp++;
+  if ((err <= 1.0) || (h <= c.hmin)) {
+    st.nacc++;
+    copy(w.ynew, w.y);
+    s.t += direction * h;
+    hnew = ros_max(c.hmin, ros_min(hnew, c.hmax));
+    if (s.reject_last) hnew = ros_min(hnew, h);
+    s.reject_last = false;
+    s.reject_more = false;
+    s.h = hnew;
+    return 1;
+  }
+  if (st.nacc >= 1) st.nrej++;
+  if (s.reject_more) hnew = h * c.facrej;
+  s.reject_more = s.reject_last;
+  s.reject_last = true;
+  s.h = hnew;
+  return 0;
+}
+
+// RosenbrockIntegrator (int/rosenbrock.c:450-627) for one cell; w.y holds
+// the cell state in and out.  Returns IERR; Texit, Hexit and the counters.
+template <int METHOD, class W>
+__device__ int integrate_cell(const CellEnv& env, W& w, const RosControls& c, double tstart,
+                              double tend, double& texit, double& hexit, Stats& st) {
+  RosState s;
+  ros_begin(env, w, c, tstart, tend, s);
+  for (;;) {
+    const int head = ros_step_head(env, w, c, s, st);
+    if (head != 0) {
+      texit = s.t;
+      hexit = s.hexit;
+      return head;
+    }
+    bool retry = false;
+    for (;;) {
+      const int r = ros_attempt<METHOD>(env, w, c, s, retry, st);
+      if (r == 1) break;
+      if (r != 0) {
+        texit = s.t;
+        hexit = s.hexit;
+        return r;
       }
     }
   }
-  texit = t;
-  return KPP_B200_IERR_SUCCESS;
 }
 
 // Rosenbrock (int/rosenbrock.c:137-446): validation and defaults, then the
 // integrator.  Returns IERR; fills stats/texit/hexit like IPAR/RPAR[10..].
 template <int METHOD, class W>
 __device__ int rosenbrock_cell(const CellEnv& env, W& w, double tstart, double tend,
-                               const double* atol, const double* rtol, const LaunchArgs& a,
-                               double rpar2, Stats& st, double& texit, double& hexit) {
-  const int* ipar = a.ipar;
-  const double* rpar = a.rpar;
-  bool autonomous = !(ipar[0] == 0);
-  bool vectortol = (ipar[1] == 0);
-  int uplimtol = vectortol ? NVAR : 1;
-  int max_no_steps = (ipar[2] == 0) ? 100000 : ipar[2];
-  if (max_no_steps < 0) return KPP_B200_IERR_MAXSTEPS_BAD;
-  if ((ipar[3] < 1) || (ipar[3] > 5)) return KPP_B200_IERR_METHOD;
-  double hmin = rpar[0];
-  if (rpar[0] < 0.0) return KPP_B200_IERR_HBOUNDS;
-  double hmax = (rpar[1] == 0.0) ? ros_abs_diff(tend, tstart)
-                                 : ros_min(ros_abs(rpar[1]), ros_abs_diff(tend, tstart));
-  if (rpar[1] < 0.0) return KPP_B200_IERR_HBOUNDS;
-  double hstart = (rpar2 == 0.0) ? ros_max(hmin, kDeltaMin)
-                                 : ros_min(ros_abs(rpar2), ros_abs_diff(tend, tstart));
-  if (rpar2 < 0.0) return KPP_B200_IERR_HBOUNDS;
-  double facmin = (rpar[3] == 0.0) ? 0.2 : rpar[3];
-  if (rpar[3] < 0.0) return KPP_B200_IERR_FACTORS;
-  double facmax = (rpar[4] == 0.0) ? 6.0 : rpar[4];
-  if (rpar[4] < 0.0) return KPP_B200_IERR_FACTORS;
-  double facrej = (rpar[5] == 0.0) ? 0.1 : rpar[5];
-  if (rpar[5] < 0.0) return KPP_B200_IERR_FACTORS;
-  double facsafe = (rpar[6] == 0.0) ? 0.9 : rpar[6];
-  if (rpar[6] < 0.0) return KPP_B200_IERR_FACTORS;
-  for (int i = 0; i < uplimtol; i++)
-    if ((atol[i] <= 0.0) || (rtol[i] <= 10.0 * kRoundoff) || (rtol[i] >= 1.0))
-      return KPP_B200_IERR_TOLERANCES;
-  return integrate_cell<METHOD>(env, w, tstart, tend, atol, rtol, autonomous, vectortol,
-                                max_no_steps, hmin, hmax, hstart, facmin, facmax, facrej,
-                                facsafe, texit, hexit, st);
+                               const LaunchArgs& a, double rpar2, Stats& st, double& texit,
+                               double& hexit) {
+  RosControls c;
+  const int bad = ros_controls(a, tstart, tend, rpar2, c);
+  if (bad) return bad;
+  return integrate_cell<METHOD>(env, w, c, tstart, tend, texit, hexit, st);
 }
 
 __device__ __forceinline__ void load_env(CellEnv& env, const double* temp, const double* cfactor,
@@ -339,19 +402,13 @@ int launch_sdirk(LaunchArgs& a, int grid, cudaStream_t s);
 // summed (INTEGRATE's Ns/Na/Nr/Ng), Texit/Hexit of the last call, IERR of the
 // first failing call (1 when every call succeeds).  Failing calls do not stop
 // the loop, as the reference driver continues after INTEGRATE reports them.
-template <int METHOD, bool CHAIN, class W>
-__device__ __forceinline__ void one_call(const LaunchArgs& a, W& w, const CellEnv& env, int cell,
-                                         int k, double& t0, double& rpar2) {
+__device__ __forceinline__ void record_call(const LaunchArgs& a, int cell, bool first, int ierr,
+                                            const Stats& st, double texit, double hexit) {
   const long ld = a.ld;
-  const double t1 = CHAIN ? t0 + a.chain_dt : a.tend[cell];
-  Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
-  double texit = 0.0, hexit = 0.0;
-  const int ierr = rosenbrock_cell<METHOD>(env, w, t0, t1, a.atol, a.rtol, a, rpar2, st, texit,
-                                           hexit);
   // y is untouched when the controls were rejected (IERR -1..-5); the
   // statistics and Texit/Hexit are then zero, as IPAR/RPAR[10..] stay.
   const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
-  if (!CHAIN || k == 0) {
+  if (first) {
     a.ierr[cell] = ierr;
 #pragma unroll
     for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
@@ -362,6 +419,16 @@ __device__ __forceinline__ void one_call(const LaunchArgs& a, W& w, const CellEn
   }
   a.rstatus[cell] = texit;
   a.rstatus[ld + cell] = hexit;
+}
+
+template <int METHOD, bool CHAIN, class W>
+__device__ __forceinline__ void one_call(const LaunchArgs& a, W& w, const CellEnv& env, int cell,
+                                         int k, double& t0, double& rpar2) {
+  const double t1 = CHAIN ? t0 + a.chain_dt : a.tend[cell];
+  Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
+  double texit = 0.0, hexit = 0.0;
+  const int ierr = rosenbrock_cell<METHOD>(env, w, t0, t1, a, rpar2, st, texit, hexit);
+  record_call(a, cell, !CHAIN || k == 0, ierr, st, texit, hexit);
   rpar2 = hexit;  // STEPMIN = RPAR[11]
   t0 = t1;        // TIME += DT
 }
@@ -377,9 +444,8 @@ __device__ __forceinline__ void one_call(const LaunchArgs& a, W& w, const CellEn
 // lanes of a warp call this together (has = false: no cell, the lane only
 // joins the barriers), and a warp barrier after each call starts the lanes'
 // next chemistry step together, so the lanes stay in the same phase of the
-// integrator instead of drifting apart over the calls; with ALIGN = false
-// (lanes that take their cells one by one) there is no barrier.
-template <int METHOD, bool CHAIN, bool ALIGN = true, class W>
+// integrator instead of drifting apart over the calls.
+template <int METHOD, bool CHAIN, class W>
 __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, int cell,
                                                      bool has = true) {
   const long ld = a.ld;
@@ -395,7 +461,7 @@ __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, 
   if (CHAIN) {
     for (int k = 0; k < a.nchain; k++) {
       if (has) one_call<METHOD, true>(a, w, env, cell, k, t0, rpar2);
-      if (ALIGN) __syncwarp();
+      __syncwarp();
     }
   } else {
     one_call<METHOD, false>(a, w, env, cell, 0, t0, rpar2);
@@ -406,6 +472,95 @@ __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, 
   }
 }
 
+// The lane-granular work queue (a.lane_queue): every lane runs its own
+// cell's chained calls as a state machine that advances by one step attempt
+// per pass of a loop the 32 lanes make together, and takes the next queue
+// position as soon as its cell is done.  The attempts (Jacobian, LU, stages,
+// error estimate: most of the work) of all lanes remain one instruction
+// stream however far apart the lanes' cells are, so no lane waits for the
+// slowest cell of its warp; what one lane does alone (loading a cell,
+// starting a call, a step's head: rates and Fun) the others wait for.  Each
+// cell's operations are integrate_cell_calls' in the same order, so results
+// are bit-identical to the other launches.
+template <int METHOD, class W>
+__device__ void integrate_refill(const LaunchArgs& a, W& w) {
+  enum { kCell, kCall, kHead, kTry };
+  const long ld = a.ld;
+  CellEnv env;
+  RosControls c;
+  RosState s;
+  Stats st = {0, 0, 0, 0, 0, 0, 0, 0};
+  int phase = kCell, cell = 0, k = 0;
+  double t0 = 0.0, t1 = 0.0, rpar2 = 0.0;
+  bool retry = false;
+  for (;;) {
+    // this lane's cell and call starts and step heads, until it has an
+    // attempt to make
+    while (phase != kTry) {
+      if (phase == kCell) {
+        const int pos = atomicAdd(a.queue, 1);
+        if (pos >= a.ncells) return;
+        cell = a.order ? a.order[pos] : pos;
+        load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, cell);
+#pragma unroll 4
+        for (int i = 0; i < NVAR; i++) w.y[i] = a.var[i * ld + cell];
+        t0 = a.tstart[cell];
+        rpar2 = a.hstart ? a.hstart[cell] : a.rpar[2];
+        k = 0;
+        phase = kCall;
+      }
+      int end = 0;  // nonzero: the call ends with this IERR
+      double texit = 0.0, hexit = 0.0;
+      if (phase == kCall) {
+        t1 = t0 + a.chain_dt;
+        st = {0, 0, 0, 0, 0, 0, 0, 0};
+        end = ros_controls(a, t0, t1, rpar2, c);
+        if (!end) {
+          ros_begin(env, w, c, t0, t1, s);
+          phase = kHead;
+        }
+      }
+      if (phase == kHead) {
+        end = ros_step_head(env, w, c, s, st);
+        if (end) {
+          texit = s.t;
+          hexit = s.hexit;
+        } else {
+          retry = false;
+          phase = kTry;
+        }
+      }
+      if (end) {
+        record_call(a, cell, k == 0, end, st, texit, hexit);
+        rpar2 = hexit;  // STEPMIN = RPAR[11]
+        t0 = t1;        // TIME += DT
+        if (++k < a.nchain) {
+          phase = kCall;
+        } else {
+#pragma unroll 4
+          for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+          phase = kCell;
+        }
+      }
+    }
+    const int r = ros_attempt<METHOD>(env, w, c, s, retry, st);
+    if (r == 1) {
+      phase = kHead;
+    } else if (r != 0) {
+      record_call(a, cell, k == 0, r, st, s.t, s.hexit);
+      rpar2 = s.hexit;
+      t0 = t1;
+      if (++k < a.nchain) {
+        phase = kCall;
+      } else {
+#pragma unroll 4
+        for (int i = 0; i < NVAR; i++) a.var[i * ld + cell] = w.y[i];
+        phase = kCell;
+      }
+    }
+  }
+}
+
 // QUEUE = false: one thread slot integrates cells slot, slot + nslots, ...
 // (grid-stride), one call each.  QUEUE = true: each warp takes the next 32
 // queue positions from the device counter until the queue is empty
@@ -413,8 +568,7 @@ __device__ __forceinline__ void integrate_cell_calls(const LaunchArgs& a, W& w, 
 // chained calls of each cell.  A queue ordered by decreasing cost hands the
 // long cells out first and keeps the 32 cells of a warp of similar cost.
 // With a.lane_queue each lane instead takes the next single position as soon
-// as its previous cell is done, so no lane waits for the slowest cell of its
-// warp (the lanes then run different cells' phases side by side).
+// as its previous cell is done (integrate_refill).
 template <int METHOD, bool QUEUE>
 __global__ void
 #if KPP_MIN_BLOCKS > 0
@@ -426,11 +580,7 @@ rosenbrock_kernel(const LaunchArgs a) {
   const long slot = (long)blockIdx.x * blockDim.x + threadIdx.x;
   Work w(a.scratch, a.nslots, slot);
   if (QUEUE && a.lane_queue) {
-    for (;;) {
-      const int pos = atomicAdd(a.queue, 1);
-      if (pos >= a.ncells) break;
-      integrate_cell_calls<METHOD, true, false>(a, w, a.order ? a.order[pos] : pos);
-    }
+    integrate_refill<METHOD>(a, w);
   } else if (QUEUE) {
     const int lane = threadIdx.x & 31;
     for (;;) {

@@ -289,10 +289,10 @@ __device__ int integrate(const CellEnv& env, W& w, const Method& m, double tinit
           if (theta < 0.99) {
             newton_rate = theta / (1.0 - theta);
             const double predicted =
-                newton_increment * pow(theta, (newton_maxit - (it + 1)) / (1.0 - theta));
+                newton_increment * KPP_POW(theta, (newton_maxit - (it + 1)) / (1.0 - theta));
             if (predicted >= newton_tol) {
               const double qn = ros_min(10.0, predicted / newton_tol);
-              fac = 0.8 * pow(qn, (-1.0 / (1 + newton_maxit - it + 1)));
+              fac = 0.8 * KPP_POW(qn, (-1.0 / (1 + newton_maxit - it + 1)));
               break;
             }
           } else {
@@ -321,7 +321,7 @@ __device__ int integrate(const CellEnv& env, W& w, const Method& m, double tinit
       if (m.E[i] != 0.0) axpy(m.E[i], w.z[i], w.tmp);
     solve(h, m.gamma, w, 1, st);
     const double err = error_norm(w.tmp, w.scal);
-    double fac = facsafe * pow(err, (-1.0 / m.elo));
+    double fac = facsafe * KPP_POW(err, (-1.0 / m.elo));
     fac = ros_max(facmin, ros_min(facmax, fac));
     double hnew = h * fac;
 

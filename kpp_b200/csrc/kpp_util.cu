@@ -1,6 +1,8 @@
 // Measurement helpers for the benchmark: the FP64 peak of this GPU, measured
-// with a throughput kernel (no vendor figure for FP64 is assumed); and the
-// device self-test of kpp_div.cuh's division through a reciprocal.
+// with a throughput kernel (no vendor figure for FP64 is assumed); the device
+// self-test of kpp_div.cuh's division through a reciprocal; and a batched
+// evaluation of the controllers' pow (kpp_ratelaws.cuh's kpp_pow_cr) beside
+// the CUDA math library's, for their tests.
 //
 //   kind 0: fused multiply-add (DFMA), 2 flops per instruction
 //   kind 1: separate multiply and add (DMUL + DADD), 1 flop per instruction;
@@ -12,6 +14,7 @@
 #include <cstdio>
 
 #include "kpp_div.cuh"
+#include "kpp_ratelaws.cuh"
 
 namespace {
 
@@ -84,9 +87,32 @@ __global__ void __launch_bounds__(256) division_check_kernel(uint64_t seed, long
   if (local) atomicAdd(bad, local);
 }
 
+__global__ void __launch_bounds__(256) pow_kernel(long long n, const double* x, const double* y,
+                                                  double* out, int which) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = which == 0 ? kpp_pow_cr(x[i], y[i]) : pow(x[i], y[i]);
+}
+
 }  // namespace
 
 extern "C" {
+
+// out[i] = x[i]^y[i] for i < n (device arrays, asynchronous on `stream`):
+// which 0, kpp_pow_cr (the integrators' controllers); 1, the CUDA math
+// library's pow.  0 on success, -1 on a bad argument or launch error.
+int kpp_b200_pow_batch(long long n, const double* x, const double* y, double* out, int which,
+                       void* stream) {
+  if (n < 0 || (which != 0 && which != 1) || (n > 0 && (!x || !y || !out))) return -1;
+  if (n == 0) return 0;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long blocks = (n + 255) / 256;
+  pow_kernel<<<(int)(blocks < sms * 8LL ? blocks : sms * 8LL), 256, 0, (cudaStream_t)stream>>>(
+      n, x, y, out, which);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 // Self-test of the division through a reciprocal (kpp_div.cuh): the number of
 // n samples (operand exponents in [emin, emax], the given mode) for which it

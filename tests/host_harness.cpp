@@ -17,11 +17,21 @@ using std::fma;
 using std::log10;
 using std::pow;
 using std::rint;
+using std::fabs;
+using std::fmod;
+using std::frexp;
+using std::isinf;
+using std::ldexp;
+using std::trunc;
+using std::sqrt;
 #define KPP_SUN_COS cos
+#define KPP_POW pow
 #include "kpp_ratelaws.cuh"
 
 // the device cosine of Update_SUN, for its own test
 extern "C" double host_cos_cr(double x) { return kpp_cos_cr(x); }
+// the device pow of the integrators' controllers, for its own test
+extern "C" double host_pow_cr(double x, double y) { return kpp_pow_cr(x, y); }
 #include KPP_MECH_HEADER
 #ifdef KPP_ADJ_HEADER
 #include KPP_ADJ_HEADER

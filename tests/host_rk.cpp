@@ -21,7 +21,14 @@ using std::log10;
 using std::pow;
 using std::rint;
 using std::sqrt;
+using std::fabs;
+using std::fmod;
+using std::frexp;
+using std::isinf;
+using std::ldexp;
+using std::trunc;
 #define KPP_SUN_COS cos
+#define KPP_POW pow
 #include "kpp_ratelaws.cuh"
 #include KPP_MECH_HEADER
 #include KPP_CMPLX_HEADER

@@ -15,7 +15,15 @@ using std::fma;
 using std::log10;
 using std::pow;
 using std::rint;
+using std::fabs;
+using std::fmod;
+using std::frexp;
+using std::isinf;
+using std::ldexp;
+using std::trunc;
+using std::sqrt;
 #define KPP_SUN_COS cos
+#define KPP_POW pow
 #include ROUTE_INCLUDES
 
 namespace {

@@ -84,6 +84,8 @@ MAX_ENV_FRACTION = 0.10
 
 def assert_var_parity(gpu, ref, alt, what="", max_env_fraction=MAX_ENV_FRACTION):
     r = var_parity(gpu, ref, alt)
+    print(f"\n[parity] {what}: largest relative error {r['well']:.3g}; {r['n_env']} of "
+          f"{r['n']} entries beyond 1e-9 within the envelope")
     assert r["ratio"] <= 1.0, f"{what}: {r}"
     assert r["n_env"] <= max_env_fraction * max(r["n"], 1), \
         f"{what}: {r['n_env']} of {r['n']} entries need the rounding envelope"

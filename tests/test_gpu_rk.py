@@ -84,6 +84,8 @@ def check(got, ref, alt, what, atol, rtol, seq_frac=0.95):
     rtol = np.asarray(rtol, dtype=np.float64).reshape(-1, 1)
     scale = atol + rtol * np.abs(var_ref)
     dist = np.sqrt(np.mean(((var - var_ref) / scale) ** 2, axis=0))
+    print(f"\n[rk bar] {what}: {same.mean():.4f} of {same.size} cells keep the sequence; "
+          f"largest error-norm distance {dist.max():.3g}")
     assert dist.max() <= SEQ_NORM_TOL, f"{what}: error-norm distance {dist.max():.3g}"
     assert same.mean() >= seq_frac, f"{what}: {same.mean():.3f} of cells keep the sequence"
     ok = ierr_ref == 1
