@@ -355,6 +355,9 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     if args.kernel == "auto":
         from kpp_b200 import autotune
         shape = autotune.apply(mech, args.workload)  # tuned on this GPU, if recorded
+    if args.queue != "tuned":
+        mech.set_queue_lanes(args.queue == "lanes")  # an explicit choice wins
+    queue = "lanes" if mech.queue_lanes() else "warps"
     kernel = mech.kernel()
     wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=shard_seed(rank))
     n = wl.ncells
@@ -644,7 +647,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
             "speedup_vs_plain": learned.value / plain.value,
             "queue_cell_order": None if queued is None else {
                 "what": "kpp_b200_rosenbrock_chain, Hstart = STEPMIN, cells in batch order "
-                        f"({args.queue} queue): the work queue without the scheduler",
+                        f"({queue} queue): the work queue without the scheduler",
                 "value": queued.value, "speedup_vs_plain": queued.value / plain.value,
                 "bit_identical_to_plain": bool(np.array_equal(queued.var_out, plain.var_out)
                                                and np.array_equal(queued.ierr, plain.ierr)),
@@ -716,7 +719,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                                f"{wl.rtol[0]:g} ATOL {wl.atol[0]:g}",
                    "mode": args.mode, "cells_per_gpu": n, "chemistry_step_s": wl.dt,
                    "method": method_name, "scheduler": sched_block["kind"],
-                   "queue": args.queue,
+                   "queue": queue,
                    "parallelism": f"cell shards x{world}",
                    "kernel": {"thread": "thread per cell", "warp": "warp per cell"}[kernel],
                    "launch_shape": shape or {"kernel": kernel, "blocks_per_sm": 0,
@@ -765,6 +768,7 @@ def run_diurnal(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
+    mech.set_queue_lanes(args.queue == "lanes")
     # saprc99: the uneven-stiffness classes; another mechanism: its own
     # workload (small_strato: 72 x 1200 s steps of 4096 cells is config 1)
     wname = (args.workload if args.workload.endswith("classes") or args.mech != "saprc99"
@@ -900,6 +904,7 @@ def run_diurnal(args, rank, world, local_rank):
                                + f"{ncalls} x {wl.dt:.0f} s Rodas3 steps, RTOL {wl.rtol[0]:g} "
                                  f"ATOL {wl.atol[0]:g}; one step = one diurnal loop of every cell",
                    "cells_per_gpu": n, "graph": "both forms replayed from CUDA graphs",
+                   "queue": "lanes" if mech.queue_lanes() else "warps",
                    "l2": ("inputs smaller than L2: 256 MB written between timed loops, "
                           "outside the timed events" if small else "inputs larger than L2")},
         "impl": "kpp_b200", "gpu_launches": args.steps,
@@ -1136,9 +1141,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--kernel", choices=["auto", "thread", "warp"], default="auto")
-    ap.add_argument("--queue", choices=["lanes", "warps"], default="warps",
-                    help="work-queue granularity of the learned and ceiling arms: each warp "
-                         "takes 32 cells at a time, or each lane one (measured equal)")
+    ap.add_argument("--queue", choices=["tuned", "lanes", "warps"], default="tuned",
+                    help="work-queue granularity of the queue, learned and ceiling arms: each "
+                         "warp takes 32 cells at a time, or each lane one (its cells advancing "
+                         "step by step together); default: the autotuner's record, else warps")
     ap.add_argument("--scheduler", choices=["learned", "plain"], default="learned")
     ap.add_argument("--weights", default=None, help="trained scheduler (.npz)")
     ap.add_argument("--accuracy-cells", type=int, default=4096,

@@ -5,7 +5,9 @@
 Measures, on a sample of the workload on the current GPU, every candidate
 launch shape of the integration: the kernel (one thread per cell, or one
 warp per cell where the mechanism has the shared-memory form) and, for the
-thread kernel, the number of 128-thread blocks kept resident per SM.  Each
+thread kernel, the number of 128-thread blocks kept resident per SM and, on
+the work-queue path, the queue's granularity (32 cells per warp, or one cell
+per lane with the lanes' cells advancing step by step together).  Each
 candidate runs the same cells the way the benchmark does (the learned
 scheduler's plan and the work-queue launch when trained weights exist, the
 plain launch otherwise); all candidates must give bit-identical results.
@@ -49,14 +51,17 @@ def apply(mech, workload: str) -> Optional[dict]:
     choice = rec["choice"]
     mech.set_kernel(choice["kernel"])
     mech.set_blocks_per_sm(choice["blocks_per_sm"])
+    if "queue" in choice:
+        mech.set_queue_lanes(choice["queue"] == "lanes")
     return dict(choice, source=str(p.relative_to(TUNING_DIR.parent.parent)))
 
 
-def candidates(mech):
-    out = [{"kernel": "thread", "blocks_per_sm": b} for b in (0, 7, 6, 5, 4)]
+def candidates(mech, queue: bool = False):
+    out = [{"kernel": "thread", "blocks_per_sm": b, "queue": q}
+           for q in (("warps", "lanes") if queue else ("warps",)) for b in (0, 7, 6, 5, 4)]
     mech.set_kernel("warp")
     if mech.kernel() == "warp":
-        out.append({"kernel": "warp", "blocks_per_sm": 0})
+        out.append({"kernel": "warp", "blocks_per_sm": 0, "queue": "warps"})
     mech.set_kernel("auto")
     return out
 
@@ -83,6 +88,7 @@ def tune(mech_name: str, workload: str, ncells: int = 1 << 18, reps: int = 2,
     def run(shape):
         mech.set_kernel(shape["kernel"])
         mech.set_blocks_per_sm(shape["blocks_per_sm"])
+        mech.set_queue_lanes(shape["queue"] == "lanes")
         best, out = None, None
         for _ in range(reps):
             v = D(wl.var)
@@ -102,7 +108,7 @@ def tune(mech_name: str, workload: str, ncells: int = 1 << 18, reps: int = 2,
         return best, out
 
     table, ref = [], None
-    for shape in candidates(mech):
+    for shape in candidates(mech, queue=sched is not None):
         ms, v = run(shape)
         same = True if ref is None else bool(torch.equal(v, ref))
         ref = v if ref is None else ref
@@ -111,12 +117,14 @@ def tune(mech_name: str, workload: str, ncells: int = 1 << 18, reps: int = 2,
             print(json.dumps(table[-1]), flush=True)
     mech.set_kernel("auto")
     mech.set_blocks_per_sm(0)
+    mech.set_queue_lanes(False)
     if not all(t["identical"] for t in table):
         raise RuntimeError("launch shapes gave different results")
     best = min(table, key=lambda t: t["ms"])
     rec = {"device": torch.cuda.get_device_name(), "mechanism": mech_name, "workload": workload,
            "sample_cells": ncells, "path": "learned plan + work queue" if sched else "plain",
-           "choice": {"kernel": best["kernel"], "blocks_per_sm": best["blocks_per_sm"]},
+           "choice": {"kernel": best["kernel"], "blocks_per_sm": best["blocks_per_sm"],
+                      "queue": best["queue"]},
            "table": table}
     if write:
         TUNING_DIR.mkdir(exist_ok=True)

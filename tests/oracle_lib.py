@@ -11,9 +11,11 @@ cell index fastest).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -93,8 +95,9 @@ class OracleLib:
         rst = np.zeros((2, ld), np.float64)
         ierr = np.zeros(ld, np.int32)
         fn = self.lib.kppref_integrate if which == "ref" else self.lib.kppor_integrate
-        fn(ld, ld, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun), _p(tstart), _p(tend),
-           _p(atol), _p(rtol), _p(ip), _p(rp), _p(hstart), _p(ist), _p(rst), _p(ierr))
+        with quiet_stdout():
+            fn(ld, ld, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun), _p(tstart), _p(tend),
+               _p(atol), _p(rtol), _p(ip), _p(rp), _p(hstart), _p(ist), _p(rst), _p(ierr))
         return var, ist, rst, ierr
 
     def set_sun_ulps(self, u: int):
@@ -176,6 +179,27 @@ def rk_lib_path(mech: str, opt: str = "") -> Path:
     return integrator_lib_path("rk", mech, opt)
 
 
+@contextlib.contextmanager
+def quiet_stdout():
+    """The reference integrators print a message per failing cell
+    (ros_ErrorMsg and its SDIRK / Runge-Kutta counterparts); error-path tests
+    make hundreds of thousands of them.  Sends the C library's stdout to
+    /dev/null for the length of a call."""
+    libc = ctypes.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(null)
+
+
 class IntegratorOracle:
     """The reference's own C SDIRK (int/sdirk.c) or Runge-Kutta
     (int/runge_kutta.c) integrator on the mechanism's generated model, per
@@ -221,9 +245,10 @@ class IntegratorOracle:
         ist = np.zeros((8, n), np.int32)
         rst = np.zeros((3, n))
         ierr = np.zeros(n, np.int32)
-        self._integrate(n, n, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun), _p(tstart),
-                        _p(tend), _p(atol), _p(rtol), _p(ic), _p(rc), _p(ist), _p(rst),
-                        _p(ierr))
+        with quiet_stdout():
+            self._integrate(n, n, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun),
+                            _p(tstart), _p(tend), _p(atol), _p(rtol), _p(ic), _p(rc), _p(ist),
+                            _p(rst), _p(ierr))
         return var, ist, rst, ierr
 
 

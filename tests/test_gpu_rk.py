@@ -8,9 +8,10 @@ driven cell by cell (oracle/refkpp/batch_driver_rk.c).
 The bar.  IERR identical for every cell.  The integrator takes discrete
 decisions on pow() results (accept the step, reuse the LU when the new step
 is within Qmin..Qmax of the old, Newton converged), so a last-ulp difference
-of pow -- CUDA's against glibc's, or glibc's against another valid rounding
--- can change a cell's step sequence (a host build of this integrator whose
-pow is one ulp off in a direction varying from call to call shows the same).
+of pow can change a cell's step sequence (a host build of this integrator
+whose pow is one ulp off in a direction varying from call to call shows the
+same).  The device's controllers use a correctly rounded pow (kpp_pow_cr),
+so they decide as the reference does wherever glibc's pow rounds correctly.
 Cells whose integrator statistics (ISTATUS) equal the reference's took the
 same step sequence: for them the bar of the other integrators holds
 (concentrations within 1e-9 relative, or within 30x the reference's own
@@ -18,8 +19,9 @@ spread under valid last-ulp roundings).  Every other cell took another valid
 sequence and must agree with the reference within SEQ_NORM_TOL of the
 integrator's own error norm (sqrt(mean(((gpu - ref) / (ATOL + RTOL |ref|))^2)),
 the norm its accept test compares with 1); such cells must stay rare
-(>= 95 % of cells keep the sequence, except on Lobatto-3A's short windows,
-where nearly every decision sits on a pow result).
+(>= 99 % of cells keep the sequence; measured: all of them, except on
+Lobatto-3A's 1e-6 s windows with the SDIRK error estimator, where 40 % do and
+nearly every decision sits on a pow result of glibc's own rounding).
 """
 import numpy as np
 import pytest
@@ -70,10 +72,11 @@ def run_both(mech, ncells, seed, ic, rc, atol=None, rtol=None, step=0, window=No
     return got, ref, alt, atol, rtol
 
 
-SEQ_NORM_TOL = 1e-2  # observed on the host: <= 4e-7
+# observed on the GPU with the controllers' correctly rounded pow: <= 9e-9
+SEQ_NORM_TOL = 1e-6
 
 
-def check(got, ref, alt, what, atol, rtol, seq_frac=0.95):
+def check(got, ref, alt, what, atol, rtol, seq_frac=0.99):
     var, ist, rst, ierr = got
     var_ref, ist_ref, rst_ref, ierr_ref = ref
     np.testing.assert_array_equal(ierr, ierr_ref, err_msg=what)
@@ -106,7 +109,9 @@ def test_every_rk_method_matches_reference(method, sdirk_error):
 def test_lobatto3a_short_windows_match_reference(sdirk_error, window):
     ic, rc = rk_controls(method=5, sdirk_error=sdirk_error)
     got, ref, alt, atol, rtol = run_both("small_strato", 128, 11, ic, rc, window=window)
-    check(got, ref, alt, f"lobatto3a {sdirk_error}", atol, rtol, seq_frac=0.0)
+    # measured: 0.40 (SDIRK estimator, 1e-6 s windows) and 1.0 of the cells
+    check(got, ref, alt, f"lobatto3a {sdirk_error}", atol, rtol,
+          seq_frac=0.25 if sdirk_error else 0.99)
 
 
 @pytest.mark.parametrize("step", [0, 3, 6])

@@ -74,7 +74,7 @@ def run_both(mech, ncells, seed, ic, rc, atol=None, rtol=None, step=0, var0=None
     return got, ref, alt
 
 
-def check(got, ref, alt, what, stats_frac=0.95):
+def check(got, ref, alt, what, stats_frac=0.99):
     var, ist, rst, ierr = got
     var_ref, ist_ref, rst_ref, ierr_ref = ref
     np.testing.assert_array_equal(ierr, ierr_ref, err_msg=what)
