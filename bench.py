@@ -350,7 +350,6 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
     mech.set_kernel(args.kernel)
-    mech.set_queue_lanes(args.queue == "lanes")
     shape = None
     if args.kernel == "auto":
         from kpp_b200 import autotune
@@ -768,7 +767,8 @@ def run_diurnal(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     mech = load(args.mech)
-    mech.set_queue_lanes(args.queue == "lanes")
+    if args.queue != "tuned":
+        mech.set_queue_lanes(args.queue == "lanes")
     # saprc99: the uneven-stiffness classes; another mechanism: its own
     # workload (small_strato: 72 x 1200 s steps of 4096 cells is config 1)
     wname = (args.workload if args.workload.endswith("classes") or args.mech != "saprc99"
@@ -1144,7 +1144,8 @@ def main():
     ap.add_argument("--queue", choices=["tuned", "lanes", "warps"], default="tuned",
                     help="work-queue granularity of the queue, learned and ceiling arms: each "
                          "warp takes 32 cells at a time, or each lane one (its cells advancing "
-                         "step by step together); default: the autotuner's record, else warps")
+                         "step by step together); default: the autotuner's record, else the "
+                         "library's default (lanes)")
     ap.add_argument("--scheduler", choices=["learned", "plain"], default="learned")
     ap.add_argument("--weights", default=None, help="trained scheduler (.npz)")
     ap.add_argument("--accuracy-cells", type=int, default=4096,

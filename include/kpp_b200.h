@@ -299,8 +299,8 @@ int kpp_b200_set_kernel(int which);
 int kpp_b200_get_kernel(void);
 
 /* Work-queue granularity of kpp_b200_rosenbrock_chain on the thread-per-cell
- * kernel (process-wide): 0 (the default) each warp takes the next 32 queue
- * positions and its lanes start every chained call together; 1 each lane
+ * kernel (process-wide): 0 each warp takes the next 32 queue positions and
+ * its lanes start every chained call together; 1 (the default) each lane
  * takes the next single position as soon as its previous cell is done, and
  * the lanes' cells advance together one step attempt at a time however far
  * apart they are, so no lane idles until the slowest cell of its warp

@@ -117,7 +117,7 @@ def tune(mech_name: str, workload: str, ncells: int = 1 << 18, reps: int = 2,
             print(json.dumps(table[-1]), flush=True)
     mech.set_kernel("auto")
     mech.set_blocks_per_sm(0)
-    mech.set_queue_lanes(False)
+    mech.set_queue_lanes(True)  # the library's default
     if not all(t["identical"] for t in table):
         raise RuntimeError("launch shapes gave different results")
     best = min(table, key=lambda t: t["ms"])

@@ -769,8 +769,9 @@ thread_local char g_last_error[512] = "";
 // constants are fixed for the call; the others always use the thread kernel.
 int g_kernel_choice = 0;
 // Work-queue granularity of the chained entry's thread-per-cell kernel: 0 a
-// warp takes 32 cells at a time, 1 each lane takes one cell at a time.
-std::atomic<int> g_lane_queue{0};
+// warp takes 32 cells at a time, 1 (the default: measured faster on every
+// workload) each lane takes one cell at a time.
+std::atomic<int> g_lane_queue{1};
 // The automatic choice runs launches of at most this many cells on the
 // warp-per-cell kernel: the thread-per-cell kernel needs about 150k cells to
 // fill a B200 and is far slower below that, while the warp-per-cell kernel

@@ -153,8 +153,8 @@ class Mechanism:
     def set_queue_lanes(self, per_lane: bool):
         """Work-queue granularity of rosenbrock_chain: each lane takes one
         cell at a time and the lanes' cells advance one step attempt at a
-        time together (True), or each warp takes 32 cells (False, the
-        default).  Results are the same bit for bit."""
+        time together (True, the default), or each warp takes 32 cells
+        (False).  Results are the same bit for bit."""
         self._check(self.lib.kpp_b200_set_queue_lanes(1 if per_lane else 0))
 
     def queue_lanes(self) -> bool:

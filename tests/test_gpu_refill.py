@@ -41,7 +41,7 @@ def run_both(m, wl, ipar, rpar, ncalls, order=None, hstart=None, dt=None, atol=N
             torch.cuda.synchronize()
             out.append([x.cpu().numpy() for x in (var, r.istatus, r.rstatus, r.ierr)])
         finally:
-            m.set_queue_lanes(False)
+            m.set_queue_lanes(True)  # the default
             m.set_kernel("auto")
     for x, y, nm in zip(out[0], out[1], ("var", "istatus", "rstatus", "ierr")):
         np.testing.assert_array_equal(x, y, err_msg=nm)
@@ -129,5 +129,5 @@ def test_fewer_cells_than_lanes_and_empty_batch():
         torch.cuda.synchronize()
         assert r.ierr.numel() == 0
     finally:
-        m.set_queue_lanes(False)
+        m.set_queue_lanes(True)  # the default
         m.set_kernel("auto")
