@@ -144,9 +144,10 @@ def make_home(kpp_home: str) -> Path:
     return home
 
 
-def generate(mech: str, kpp_home: str, force: bool = False) -> Path:
+def generate(mech: str, kpp_home: str, force: bool = False, hessian: bool = True) -> Path:
     """Run the generator with #LANGUAGE CUDA on one of KPP's models; returns
-    the output directory (with route_includes.h)."""
+    the output directory (with route_includes.h).  hessian: #HESSIAN ON (the
+    Hessian, Hess_Vec and HessTR_Vec of the discrete adjoint)."""
     exe = build_generator(kpp_home, force)
     home = make_home(kpp_home)
     out = BUILD / "out" / mech
@@ -162,7 +163,8 @@ def generate(mech: str, kpp_home: str, force: bool = False) -> Path:
         model = "#INCLUDE    mcm_isoprene_c.eqn\n"
     (out / f"{mech}.kpp").write_text(
         f"#LANGUAGE   CUDA\n#DOUBLE     ON\n#INTEGRATOR none\n"
-        f"#DRIVER     none\n#JACOBIAN   SPARSE_LU_ROW\n#HESSIAN    OFF\n#STOICMAT   OFF\n"
+        f"#DRIVER     none\n#JACOBIAN   SPARSE_LU_ROW\n#HESSIAN    {'ON' if hessian else 'OFF'}\n"
+        f"#STOICMAT   OFF\n"
         f"#MEX        OFF\n" + model)
     r = subprocess.run([str(exe), f"{mech}.kpp"], cwd=out, env={**os.environ, "KPP_HOME": str(home)},
                        stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
@@ -179,8 +181,12 @@ def generate(mech: str, kpp_home: str, force: bool = False) -> Path:
              "// Generated by kpp_b200/kppgen/build.py.  Do not edit.", "#pragma once",
              f'#include "{mech}_Parameters.h"', f'#include "{mech}_JacobianSP.cu"',
              f'#include "{mech}_Function.cu"', f'#include "{mech}_Jacobian.cu"',
-             f'#include "{mech}_LinearAlgebra.cu"', f'#include "{mech}_Rates.cu"',
-             "// the sizes are kpp_b200's own constants from here on"]
+             f'#include "{mech}_LinearAlgebra.cu"', f'#include "{mech}_Rates.cu"']
+    nhess = re.search(r"^#define\s+NHESS\s+(\d+)", params, flags=re.M)
+    if hessian and nhess:
+        lines += [f'#include "{mech}_HessianSP.cu"', f'#include "{mech}_Hessian.cu"',
+                  f"#define KPP_NHESS {nhess.group(1)}  // entries of the sparse Hessian"]
+    lines += ["// the sizes are kpp_b200's own constants from here on"]
     lines += [f"#undef {m}" for m in macros]
     (out / "route_includes.h").write_text("\n".join(lines) + "\n")
     return out

@@ -17,6 +17,8 @@
 #                                                 SDIRK integrator (int/sdirk.c)
 #   oracle/_ref/<mech>_rk/libkpprk_<mech>[_O3|_pw].so  ... with the reference Runge-Kutta
 #                                                 integrator (int/runge_kutta.c)
+#   oracle/_ref/<mech>_adj/libkppadj_<mech>[_O3|_pw].so  ... with the reference Rosenbrock
+#                                                 adjoint (int/rosenbrock_adj.c) and Hessian
 #
 # The generator is compiled from the unchanged sources in $KPP_REF/src; only
 # the flex/bison front end is replaced by kpp_b200/kppgen/frontend.c because
@@ -51,7 +53,7 @@ done
 "$CC" "$OUT"/obj/*.o -lm -o "$OUT/kpp"
 
 # ---- 2. per-mechanism reference model ---------------------------------------
-# build_integrator_model MECH INTEGRATOR DRIVER TAG PREFIX: the model with
+# build_integrator_model MECH INTEGRATOR DRIVER TAG PREFIX [HESSIAN]: the model with
 # another reference integrator and its batch driver (refkpp/DRIVER.c) in
 # oracle/_ref/MECH_TAG/: libPREFIX_MECH.so (reference flags), _O3 (FMA
 # contraction) and _pw (the integrator's pow() through the driver's
@@ -59,7 +61,7 @@ done
 # refkpp/cos_knob.h; each can move its result one ulp: other valid
 # roundings of pow and cos).
 build_integrator_model() {
-  local mech="$1" integ="$2" driver="$3" tag="$4" prefix="$5"
+  local mech="$1" integ="$2" driver="$3" tag="$4" prefix="$5" hessian="${6:-OFF}"
   local ds="$OUT/${mech}_${tag}"
   local model="#MODEL      $mech"
   rm -rf "$ds"
@@ -76,7 +78,7 @@ $model
 #INTEGRATOR $integ
 #DRIVER     $HERE/refkpp/$driver
 #JACOBIAN   SPARSE_LU_ROW
-#HESSIAN    OFF
+#HESSIAN    $hessian
 #STOICMAT   OFF
 #MEX        OFF
 #INLINE C_GLOBAL
@@ -188,5 +190,10 @@ EOF
   # entries' parity tests
   build_integrator_model "$mech" sdirk batch_driver_sdirk sdirk kppsd
   build_integrator_model "$mech" runge_kutta batch_driver_rk rk kpprk
+  # and with the reference Rosenbrock adjoint (int/rosenbrock_adj.c), which
+  # needs the generated Hessian (not for MCM: its Hessian is not built)
+  if [ "$mech" != "mcm_isoprene" ]; then
+    build_integrator_model "$mech" rosenbrock_adj batch_driver_adj adj kppadj ON
+  fi
   echo "$SRC_KEY" > "$OUT/$mech.stamp"
 done
