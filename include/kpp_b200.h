@@ -161,6 +161,34 @@ int kpp_b200_runge_kutta_host(int ncells, int ld, double *var, const double *fix
                               const double *rtol, const int *icntrl, const double *rcntrl,
                               int *istatus, double *rstatus, int *ierr, int chunk);
 
+/* The Rosenbrock discrete adjoint, RosenbrockADJ (int/rosenbrock_adj.c:191-597)
+ * per cell, replacing the model's INTEGRATE_ADJ loop over cells
+ * (drv/general_adj.c): a forward Rosenbrock integration of var from tstart[c]
+ * to tend[c] that keeps each accepted step (T, H, stage states, stage
+ * vectors, and the factorised matrix when ICNTRL[7] != 0) in the cell's
+ * trajectory, then the backward pass over it that updates the nadj adjoint
+ * vectors in lambda[nadj * NVAR][ld] (adjoint m's entry i in row
+ * m * NVAR + i) in place.  ICNTRL / RCNTRL in the C layout of
+ * int/rosenbrock_adj.c (method ICNTRL[2]: 0/4 Rodas3, 1 Ros2, 2 Ros3, 3 Ros4,
+ * 5 Rodas4, 7 Rodas3_1; ICNTRL[6]: 0/2 discrete adjoint, 1 forward only; 3
+ * and 4, the continuous adjoints, are not built: EINVAL).  bufsize is the
+ * trajectory capacity per cell, the reference's `bufsize` global: the step
+ * limit is bufsize - 1, and any ICNTRL[3] != 0 returns IERR -1, as in the
+ * reference.  work: a device buffer of at least
+ * kpp_b200_rosenbrock_adj_work_bytes(ld, nadj, bufsize, ICNTRL[7]) bytes.
+ * Outputs: istatus[8][ld] = ISTATUS[1..8] (forward and backward counters),
+ * rstatus[3][ld] = Texit, Hexit, Hnew; ierr[ld].  Only in the libraries
+ * built on KPP's own generator with the Hessian
+ * (libkpp_b200_<mech>_kpproute.so); elsewhere EINVAL.  Asynchronous on
+ * `stream`.  No single counterpart: the batched form of RosenbrockADJ. */
+size_t kpp_b200_rosenbrock_adj_work_bytes(int ld, int nadj, int bufsize, int save_lu);
+int kpp_b200_rosenbrock_adj(int ncells, int ld, double *var, const double *fix,
+                            const double *temp, const double *cfactor, const double *sun,
+                            const double *tstart, const double *tend, const double *atol,
+                            const double *rtol, int nadj, double *lambda, const int *icntrl,
+                            const double *rcntrl, int bufsize, double *work, size_t work_bytes,
+                            int *istatus, double *rstatus, int *ierr, void *stream);
+
 /* The host model's time loop (drv/general.c:59-76) over INTEGRATE
  * (int/rosenbrock.c:94-133) for every cell in one persistent launch: each cell
  * makes ncalls consecutive calls Rosenbrock(T, T + dt) with T = tstart[c]

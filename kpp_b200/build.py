@@ -50,6 +50,7 @@ NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-
 METHOD_PARTS = [1, 2, 3, 4, 5]
 SDIRK_PART = 6  # the SDIRK integrator
 RK_PART = 7     # the Runge-Kutta integrator (complex LU from <mech>_cmplx.cuh)
+ADJ_PART = 8    # the Rosenbrock discrete adjoint (generator route with the Hessian only)
 # Mechanisms at or above this LU size keep per-cell work arrays in the
 # cell-fastest global scratch layout instead of thread-local arrays.
 SCRATCH_LU_NONZERO = 200
@@ -177,6 +178,8 @@ def compile_library(mech: str, header: Path, jobs: int, force: bool = False,
     host_header = GEN_OUT / f"{mech}_host.h"
     lib = library_path(mech, "kppcu" if route_dir is None else "kpp")
     parts = [0] + METHOD_PARTS + [SDIRK_PART, RK_PART]
+    if route_dir is not None and "KPP_NHESS" in (route_dir / "route_includes.h").read_text():
+        parts.append(ADJ_PART)
 
     def part_flags(part: int):
         f = ARCH + NVCC_FLAGS + defines + [f"-DKPP_PART={part}", "-I", str(GEN_OUT)]

@@ -755,12 +755,55 @@ int launch_rk(LaunchArgs& a, int grid, cudaStream_t s) {
 }
 #endif  // KPP_PART == 7
 
+#if KPP_PART == 8
+#include "kpp_adj_int.cuh"
+
+// The Rosenbrock discrete adjoint (kpp_adj_int.cuh), one thread per cell;
+// ICNTRL / RCNTRL travel in ipar / rpar of the launch.  Each cell's work
+// arrays and trajectory are column `cell` of `work` (element e at
+// work[e * ld + cell]), so the threads of a warp touch consecutive words.
+__global__ void __launch_bounds__(128) adj_kernel(const LaunchArgs a, double* lambda, int nadj,
+                                                  int bufsize, double* work) {
+  const long cell = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= a.ncells) return;
+  const long ld = a.ld;
+  CellEnv env;
+  load_env(env, a.temp, a.cfactor, a.sun, a.fix, ld, (int)cell);
+  kpp_adj::AdjStatus st;
+  const int ierr = kpp_adj::rosenbrock_adj_cell(
+      env, a.ipar, a.rpar, a.atol, a.rtol, a.tstart[cell], a.tend[cell],
+      kpp_adj::Col{a.var + cell, ld}, kpp_adj::Col{lambda + cell, ld}, nadj, bufsize,
+      kpp_adj::Col{work + cell, ld}, st);
+  a.ierr[cell] = ierr;
+  const int sv[8] = {st.nfun, st.njac, st.nstp, st.nacc, st.nrej, st.ndec, st.nsol, st.nsng};
+#pragma unroll
+  for (int i = 0; i < 8; i++) a.istatus[i * ld + cell] = sv[i];
+  a.rstatus[cell] = st.texit;
+  a.rstatus[ld + cell] = st.hexit;
+  a.rstatus[2 * ld + cell] = st.hnew;
+}
+
+int launch_adj(LaunchArgs& a, double* lambda, int nadj, int bufsize, double* work,
+               cudaStream_t s) {
+  const int grid = (a.ncells + kBlock - 1) / kBlock;
+  adj_kernel<<<grid, kBlock, 0, s>>>(a, lambda, nadj, bufsize, work);
+  return check_launch("adj_kernel");
+}
+#endif  // KPP_PART == 8
+
 #else  // KPP_PART == 0
 
 #define KPP_RK_HOST_ONLY
 #include "kpp_rk.cuh"
 // The Runge-Kutta kernel (KPP_PART 7).
 int launch_rk(LaunchArgs& a, int grid, cudaStream_t s);
+#if defined(KPP_NHESS)
+#include "kpp_adj_int.cuh"
+// The Rosenbrock discrete adjoint kernel (KPP_PART 8), in libraries built on
+// the generator route with the Hessian.
+int launch_adj(LaunchArgs& a, double* lambda, int nadj, int bufsize, double* work,
+               cudaStream_t s);
+#endif
 
 thread_local char g_last_error[512] = "";
 
@@ -1397,6 +1440,48 @@ int kpp_b200_runge_kutta(int ncells, int ld, double* var, const double* fix,
   if (rc != KPP_B200_OK) return rc;
   a.scratch_doubles = bytes / sizeof(double);
   return launch_rk(a, (int)(a.nslots / kBlock), s);
+}
+
+size_t kpp_b200_rosenbrock_adj_work_bytes(int ld, int nadj, int bufsize, int save_lu) {
+#if defined(KPP_NHESS)
+  if (ld < 0 || nadj < 0 || bufsize < 1) return 0;
+  return (size_t)kpp_adj::adj_layout(nadj, bufsize, save_lu != 0).total * (size_t)ld *
+         sizeof(double);
+#else
+  (void)ld; (void)nadj; (void)bufsize; (void)save_lu;
+  return 0;
+#endif
+}
+
+int kpp_b200_rosenbrock_adj(int ncells, int ld, double* var, const double* fix,
+                            const double* temp, const double* cfactor, const double* sun,
+                            const double* tstart, const double* tend, const double* atol,
+                            const double* rtol, int nadj, double* lambda, const int* icntrl,
+                            const double* rcntrl, int bufsize, double* work, size_t work_bytes,
+                            int* istatus, double* rstatus, int* ierr, void* stream) {
+#if defined(KPP_NHESS)
+  LaunchArgs a;
+  int rc = fill_args(a, ncells, ld, var, fix, temp, cfactor, sun, tstart, tend, atol, rtol,
+                     icntrl, rcntrl, nullptr, istatus, rstatus, ierr);
+  if (rc != KPP_B200_OK) return rc;
+  if (nadj < 0) return fail(KPP_B200_EINVAL, "nadj must be >= 0");
+  if (bufsize < 1) return fail(KPP_B200_EINVAL, "bufsize must be >= 1");
+  if (ncells == 0) return KPP_B200_OK;
+  if (nadj > 0 && !lambda) return fail(KPP_B200_EINVAL, "null lambda");
+  if (icntrl[6] == 3 || icntrl[6] == 4)
+    return fail(KPP_B200_EINVAL, "ICNTRL[6] 3 and 4 (continuous adjoints) are not built");
+  const size_t need = kpp_b200_rosenbrock_adj_work_bytes(ld, nadj, bufsize, icntrl[7]);
+  if (!work || work_bytes < need) return fail(KPP_B200_EINVAL, "work buffer too small");
+  return launch_adj(a, lambda, nadj, bufsize, work, (cudaStream_t)stream);
+#else
+  (void)ncells; (void)ld; (void)var; (void)fix; (void)temp; (void)cfactor; (void)sun;
+  (void)tstart; (void)tend; (void)atol; (void)rtol; (void)nadj; (void)lambda; (void)icntrl;
+  (void)rcntrl; (void)bufsize; (void)work; (void)work_bytes; (void)istatus; (void)rstatus;
+  (void)ierr; (void)stream;
+  return fail(KPP_B200_EINVAL,
+              "this library has no Hessian: the adjoint is in the library built on KPP's own "
+              "generator (libkpp_b200_<mech>_kpproute.so)");
+#endif
 }
 
 int kpp_b200_rosenbrock_chain(int ncells, int ld, double* var, const double* fix,

@@ -105,6 +105,12 @@ class Mechanism:
         L.kpp_b200_runge_kutta.argtypes = L.kpp_b200_sdirk.argtypes
         L.kpp_b200_sdirk_host.argtypes = L.kpp_b200_sdirk.argtypes[:-1] + [ctypes.c_int]
         L.kpp_b200_runge_kutta_host.argtypes = L.kpp_b200_sdirk_host.argtypes
+        L.kpp_b200_rosenbrock_adj_work_bytes.argtypes = [ctypes.c_int] * 4
+        L.kpp_b200_rosenbrock_adj_work_bytes.restype = ctypes.c_size_t
+        L.kpp_b200_rosenbrock_adj.argtypes = (
+            [ctypes.c_int, ctypes.c_int] + [_vp] * 9 + [ctypes.c_int, _vp]
+            + [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_int, _vp,
+               ctypes.c_size_t] + [_vp] * 4)
         L.kpp_b200_user_species.argtypes = [_vp, _vp]
         L.kpp_b200_shuffle_user2kpp.argtypes = [ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
                                                 _vp, _vp]
@@ -363,6 +369,55 @@ class Mechanism:
             n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
             _ptr(tend), _ptr(atol), _ptr(rtol), ic, rc, _ptr(out.istatus), _ptr(out.rstatus),
             _ptr(out.ierr), _vp(s.cuda_stream)))
+        return out
+
+    def rosenbrock_adj(self, var: torch.Tensor, fix: torch.Tensor, temp: torch.Tensor,
+                       tstart: torch.Tensor, tend: torch.Tensor, atol: torch.Tensor,
+                       rtol: torch.Tensor, lam: torch.Tensor, icntrl: Sequence[int],
+                       rcntrl: Sequence[float], bufsize: int = 1000,
+                       cfactor: Optional[torch.Tensor] = None, sun: Optional[torch.Tensor] = None,
+                       ncells: Optional[int] = None, out: Optional[RosenbrockResult] = None,
+                       stream: Optional[torch.cuda.Stream] = None) -> RosenbrockResult:
+        """The reference's Rosenbrock discrete adjoint for every cell
+        (kpp_b200_rosenbrock_adj, libraries built on KPP's own generator):
+        var and lam [NADJ * NVAR, ld] in place; ICNTRL / RCNTRL in the C
+        layout of int/rosenbrock_adj.c; bufsize = trajectory entries per cell
+        (the step limit is bufsize - 1); istatus = ISTATUS[1..8], rstatus
+        [3, ld] = Texit, Hexit, Hnew.  The work buffer is allocated here.
+        Asynchronous."""
+        f64, i32 = torch.float64, torch.int32
+        self._dev(var, f64, "var")
+        self._dev(lam, f64, "lam")
+        ld = var.shape[1]
+        n = ld if ncells is None else ncells
+        for t, nm in ((fix, "fix"), (temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                      (atol, "atol"), (rtol, "rtol"), (cfactor, "cfactor"), (sun, "sun")):
+            self._dev(t, f64, nm)
+        if lam.dim() != 2 or lam.shape[1] != ld or lam.shape[0] % self.nvar:
+            raise KppError(f"lam must have shape [NADJ * {self.nvar}, {ld}], got "
+                           f"{list(lam.shape)}")
+        nadj = lam.shape[0] // self.nvar
+        self._shapes(ld, n, rows=((var, "var", self.nvar), (fix, "fix", self.nfix)),
+                     cols=((temp, "temp"), (tstart, "tstart"), (tend, "tend"),
+                           (cfactor, "cfactor"), (sun, "sun")),
+                     device=var.device, tol=(atol, rtol), vector_tol=int(icntrl[1]) == 0)
+        self._outputs(out, ld, 3, var.device)
+        if out is None:
+            out = RosenbrockResult(ierr=torch.empty(ld, dtype=i32, device=var.device),
+                                   istatus=torch.empty(8, ld, dtype=i32, device=var.device),
+                                   rstatus=torch.empty(3, ld, dtype=f64, device=var.device))
+        nbytes = int(self.lib.kpp_b200_rosenbrock_adj_work_bytes(ld, nadj, int(bufsize),
+                                                                 int(icntrl[7])))
+        work = torch.empty(max(nbytes // 8, 1), dtype=f64, device=var.device)
+        ic = (ctypes.c_int * 20)(*[int(x) for x in icntrl])
+        rc = (ctypes.c_double * 20)(*[float(x) for x in rcntrl])
+        s = stream if stream is not None else torch.cuda.current_stream(var.device)
+        self._check(self.lib.kpp_b200_rosenbrock_adj(
+            n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
+            _ptr(tend), _ptr(atol), _ptr(rtol), nadj, _ptr(lam), ic, rc, int(bufsize),
+            _ptr(work), nbytes, _ptr(out.istatus), _ptr(out.rstatus), _ptr(out.ierr),
+            _vp(s.cuda_stream)))
+        out.work = work  # kept alive until the caller drops the result
         return out
 
     def rosenbrock_chain(self, var: torch.Tensor, fix: torch.Tensor, temp: torch.Tensor,
