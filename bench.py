@@ -88,6 +88,14 @@ def _cpu_worker(args):
     null = os.open(os.devnull, os.O_WRONLY)
     os.dup2(null, 1)
     os.close(null)
+    if integ is not None and integ[0] == "adj":
+        from oracle_lib import AdjOracle
+        o = AdjOracle(mech, lib_opt)
+        lam = np.random.default_rng(7).standard_normal((integ[3] * o.nvar, sl_var.shape[1]))
+        t = time.perf_counter()
+        o.integrate(sl_var, sl_fix, temp, t0, t1, atol, rtol, lam, integ[1], integ[2], integ[4],
+                    cfactor=cf, sun=sun)
+        return time.perf_counter() - t
     if integ is not None:
         from oracle_lib import RkOracle, SdirkOracle
         o = (SdirkOracle if integ[0] == "sdirk" else RkOracle)(mech, lib_opt)
@@ -920,12 +928,185 @@ def run_diurnal(args, rank, world, local_rank):
     }
 
 
+def run_adjoint(args, rank, world, local_rank):
+    """The Rosenbrock discrete adjoint (int/rosenbrock_adj.c) on the
+    fresh-cell workload, in the library built on KPP's own generator: every
+    timed step integrates the same fresh batch forward over one chemistry
+    step and back with kpp_b200_rosenbrock_adj (one launch), NADJ adjoint
+    vectors per cell."""
+    import torch
+    from kpp_b200 import Mechanism, workloads
+    from kpp_b200 import build as kbuild
+    from kpp_b200.build import LIB
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    path = kbuild.library_path(args.mech, "kpp")
+    if not path.exists():
+        raise SystemExit(f"{path} not built: the adjoint is in the generator-route library")
+    mech = Mechanism(args.mech, path=path)
+    wl = workloads.for_mechanism(mech, args.workload, args.adj_cells, seed=shard_seed(rank))
+    n = wl.ncells
+    kind, ic, rc, nadj, bufsize = mode_integrator(args)
+    name = integrator_name(kind, ic[2])
+    D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    lam_h = np.random.default_rng(7).standard_normal((nadj * mech.nvar, n))
+    var0, lam0 = D(wl.var), D(lam_h)
+    var, lam = var0.clone(), lam0.clone()
+    fix, temp = D(wl.fix), D(wl.temp)
+    cf = D(wl.cfactor) if wl.cfactor is not None else None
+    sun = D(wl.sun) if wl.sun is not None else None
+    atol, rtol = D(wl.atol), D(wl.rtol)
+    t0, t1 = (D(x) for x in wl.step_bounds(0))
+    stream = torch.cuda.current_stream(dev)
+    work = torch.empty(int(mech.lib.kpp_b200_rosenbrock_adj_work_bytes(n, nadj, bufsize, ic[7]))
+                       // 8, dtype=torch.float64, device=dev)
+    box = [None]
+    small = wl.var.nbytes + lam_h.nbytes < (192 << 20)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if small else None
+
+    def step():
+        var.copy_(var0)
+        lam.copy_(lam0)
+        box[0] = mech.rosenbrock_adj(var, fix, temp, t0, t1, atol, rtol, lam, ic, rc,
+                                     bufsize=bufsize, cfactor=cf, sun=sun, out=box[0], work=work)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    stats = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for e0, e1 in evs:
+            var.copy_(var0)
+            lam.copy_(lam0)
+            if flush is not None:
+                flush.fill_(1)
+            e0.record(stream)
+            box[0] = mech.rosenbrock_adj(var, fix, temp, t0, t1, atol, rtol, lam, ic, rc,
+                                         bufsize=bufsize, cfactor=cf, sun=sun, out=box[0],
+                                         work=work)
+            e1.record(stream)
+            stats.append(box[0].istatus.sum(dim=1))
+        torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    if world > 1:
+        ms = reduce_max(ms, dev)
+    ist = torch.stack(stats).sum(dim=0).cpu().numpy().astype(np.int64)
+    nfun, njac, nstp, nacc, nrej, ndec, nsol, nsng = ist.tolist()
+    ierr = box[0].ierr.cpu().numpy()
+    # FP64 work from the counters, a lower bound: Fun, Jacobian, LU and
+    # (transposed) solves of both passes; the Hessian and its products are
+    # not counted
+    opsd = {}
+    hdr = REPO / "kpp_b200" / "_gen" / f"{args.mech}.cuh"
+    for line in hdr.read_text().splitlines() if hdr.exists() else []:
+        if line.startswith("#define KPP_OPS_"):
+            _, kk, v = line.split()
+            opsd[kk[8:].lower()] = int(v)
+    flops = (nfun * opsd.get("fun", 0) + njac * opsd.get("jac", 0)
+             + ndec * opsd.get("decomp", 0) + nsol * opsd.get("solve", 0))
+    achieved = flops / (ms / 1e3) / 1e12
+    peak_fma, _ = fp64_peak(LIB / "libkpp_b200_util.so")
+
+    e2e = None
+    if args.e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        h = {k: pin(v) for k, v in (("var", wl.var), ("lam", lam_h), ("fix", wl.fix),
+                                    ("temp", wl.temp), ("t0", wl.step_bounds(0)[0]),
+                                    ("t1", wl.step_bounds(0)[1]), ("atol", wl.atol),
+                                    ("rtol", wl.rtol))}
+        if wl.cfactor is not None:
+            h["cf"] = pin(wl.cfactor)
+        if wl.sun is not None:
+            h["sun"] = pin(wl.sun)
+        h_out = {"var": torch.empty_like(h["var"]).pin_memory(),
+                 "lam": torch.empty_like(h["lam"]).pin_memory(),
+                 "ist": torch.empty(8, n, dtype=torch.int32).pin_memory(),
+                 "rst": torch.empty(3, n, dtype=torch.float64).pin_memory(),
+                 "ierr": torch.empty(n, dtype=torch.int32).pin_memory()}
+        d = {k: torch.empty_like(v, device=dev) for k, v in h.items()}
+        ebox = [None]
+
+        def e2e_step():
+            for k, v in h.items():
+                d[k].copy_(v, non_blocking=True)
+            ebox[0] = o = mech.rosenbrock_adj(d["var"], d["fix"], d["temp"], d["t0"], d["t1"],
+                                              d["atol"], d["rtol"], d["lam"], ic, rc,
+                                              bufsize=bufsize, cfactor=d.get("cf"),
+                                              sun=d.get("sun"), out=ebox[0], work=work)
+            h_out["var"].copy_(d["var"], non_blocking=True)
+            h_out["lam"].copy_(d["lam"], non_blocking=True)
+            h_out["ist"].copy_(o.istatus, non_blocking=True)
+            h_out["rst"].copy_(o.rstatus, non_blocking=True)
+            h_out["ierr"].copy_(o.ierr, non_blocking=True)
+            stream.synchronize()
+
+        e2e_step()
+        torch.cuda.synchronize()
+        t_start = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        ems = (time.perf_counter() - t_start) * 1e3
+        if world > 1:
+            ems = reduce_max(ems, dev)
+        nb = lambda x: x.numel() * x.element_size()
+        e2e = {"value": whole_job_rate(n, world, args.steps, ems), "unit": UNIT,
+               "h2d_bytes_per_step": int(sum(nb(v) for v in h.values())),
+               "d2h_bytes_per_step": int(sum(nb(v) for v in h_out.values())),
+               "ms_per_step": ems / args.steps,
+               "api": "Mechanism.rosenbrock_adj (kpp_b200_rosenbrock_adj), pinned host arrays "
+                      "copied in and out every step",
+               "matches_device_run": bool(np.array_equal(h_out["lam"].numpy(),
+                                                         lam.cpu().numpy()))}
+
+    return {
+        "metric": f"{args.mech} cell-steps/s at {n} cells, Rosenbrock discrete adjoint "
+                  f"{name}, NADJ {nadj} (int/rosenbrock_adj.c)",
+        "value": whole_job_rate(n, world, args.steps, ms), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{args.mech} {args.workload} (fresh) {name} forward and "
+                               f"discrete adjoint, {n} cells per GPU, {wl.dt:.0f} s chemistry "
+                               f"step, RTOL {wl.rtol[0]:g} ATOL {wl.atol[0]:g}, NADJ {nadj}, "
+                               f"{bufsize} trajectory entries per cell",
+                   "mode": "adj", "cells_per_gpu": n, "method": name, "nadj": nadj,
+                   "bufsize": bufsize, "library": path.name,
+                   "work_bytes": int(work.numel() * 8),
+                   "parallelism": f"cell shards x{world}",
+                   "l2": ("inputs smaller than L2: 256 MB written between timed steps, outside "
+                          "the timed events" if small else "inputs larger than L2")},
+        "impl": "kpp_b200", "gpu_launches": args.steps,
+        "stats": {"internal_steps_per_cell_step": nstp / (n * args.steps),
+                  "ierr_ok_fraction": float((ierr == 1).mean()),
+                  "istatus_sum": dict(zip(["nfun", "njac", "nstp", "nacc", "nrej", "ndec",
+                                           "nsol", "nsng"], map(int, ist)))},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fma, "unit": "TFLOP/s",
+                     "frac": achieved / peak_fma if peak_fma > 0 else None, "traffic": None,
+                     "achieved_note": "lower bound: Fun, Jacobian, LU and solves of both "
+                                      "passes; Hessian evaluations and products not counted",
+                     "peak_source": "measured on this GPU by the DFMA throughput kernel "
+                                    "(kpp_b200/csrc/kpp_util.cu)"},
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }, wl
+
+
 SDIRK_NAMES = {1: "Sdirk2a", 2: "Sdirk2b", 3: "Sdirk3a", 4: "Sdirk4a", 5: "Sdirk4b"}
 RK_NAMES = {0: "Radau-2A", 1: "Radau-2A", 2: "Lobatto-3C", 3: "Gauss", 4: "Radau-1A",
             5: "Lobatto-3A"}
 # kind: (entry of kpp_b200.Mechanism, reference file, method names, default name)
+ADJ_NAMES = {0: "Rodas3", 1: "Ros2", 2: "Ros3", 3: "Ros4", 4: "Rodas3", 5: "Rodas4",
+             7: "Rodas3_1"}
 INTEGRATORS = {"sdirk": ("sdirk", "int/sdirk.c", SDIRK_NAMES, "Sdirk2a"),
-               "rk": ("runge_kutta", "int/runge_kutta.c", RK_NAMES, "Radau-2A")}
+               "rk": ("runge_kutta", "int/runge_kutta.c", RK_NAMES, "Radau-2A"),
+               "adj": ("rosenbrock_adj", "int/rosenbrock_adj.c", ADJ_NAMES, "Rodas3")}
 
 
 def integrator_controls(kind: str, method: int):
@@ -945,6 +1126,11 @@ def mode_integrator(args):
         return integrator_controls("sdirk", args.sdirk_method)
     if args.mode == "rk":
         return integrator_controls("rk", args.rk_method)
+    if args.mode == "adj":
+        # (kind, ICNTRL, RCNTRL, NADJ, bufsize): the discrete adjoint of the
+        # method, ICNTRL[3] = 0 (the step limit is bufsize - 1)
+        kind, ic, rc = integrator_controls("adj", args.adj_method)
+        return kind, ic, rc, args.nadj, args.adj_bufsize
     return None
 
 
@@ -1125,13 +1311,19 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal", "sdirk", "rk"],
+    ap.add_argument("--mode", choices=["fresh", "chain", "diurnal", "sdirk", "rk", "adj"],
                     default="fresh")
     ap.add_argument("--sdirk-method", type=int, default=0,
                     help="ICNTRL[2] of the SDIRK mode (0: INTEGRATE's default, Sdirk2a)")
     ap.add_argument("--rk-method", type=int, default=0,
                     help="ICNTRL[2] of the Runge-Kutta mode (0: INTEGRATE's default, Radau-2A)")
     ap.add_argument("--calls", type=int, default=24, help="chemistry steps of a diurnal loop")
+    ap.add_argument("--adj-method", type=int, default=0,
+                    help="--mode adj: ICNTRL[2] of int/rosenbrock_adj.c (0 Rodas3)")
+    ap.add_argument("--nadj", type=int, default=1, help="--mode adj: adjoint vectors per cell")
+    ap.add_argument("--adj-bufsize", type=int, default=200,
+                    help="--mode adj: trajectory entries per cell (step limit bufsize - 1)")
+    ap.add_argument("--adj-cells", type=int, default=32768, help="--mode adj: cells per GPU")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["kpp_b200", "reference"], default="kpp_b200")
     ap.add_argument("--mech", default="saprc99")
@@ -1172,7 +1364,8 @@ def main():
         from oracle_lib import OracleLib
         # the workload from the reference's own generated model (species,
         # #INITVALUES, CFACTOR): this arm maps no library of kpp_b200
-        wl = workloads.for_mechanism(OracleLib(args.mech), args.workload, args.ncells,
+        wl = workloads.for_mechanism(OracleLib(args.mech), args.workload,
+                                     args.adj_cells if args.mode == "adj" else args.ncells,
                                      seed=workloads.SEED_EVAL)
         integ = mode_integrator(args)
         with ctx.Pool(procs) as pool:
@@ -1196,13 +1389,16 @@ def main():
             name = integrator_name(kind, integ[1][2])
             metric = (f"{args.mech} cell-steps/s at {args.ncells} cells, {kind.upper()} {name} "
                       f"({source})")
+            if kind == "adj":
+                metric = (f"{args.mech} cell-steps/s at {args.adj_cells} cells, Rosenbrock "
+                          f"discrete adjoint {name}, NADJ {args.nadj} ({source})")
         line = {"metric": metric, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(walls),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "impl": "reference",
                 "config": {"workload": f"{args.mech} {args.workload} plain, reference controls, chemistry "
                                        f"steps, RTOL 1e-3 ATOL 1e-2; each step a sample of "
-                                       f"{n_sample} of the {args.ncells} cells"},
+                                       f"{n_sample} of the {wl.ncells} cells"},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": "reference",
                                  "sample": f"{n_sample} cells x 1 chemistry step per timed step, "
                                            f"{procs} processes, KPP-generated C + {source} "
@@ -1234,6 +1430,8 @@ def main():
             pool.close()
             pool = None
         result = run_diurnal(args, rank, world, local_rank)
+    elif args.mode == "adj":
+        result, wl = run_adjoint(args, rank, world, local_rank)
     elif integ is not None:
         result, wl = run_integrator(args, rank, world, local_rank, integ[0])
     else:

@@ -377,13 +377,15 @@ class Mechanism:
                        rcntrl: Sequence[float], bufsize: int = 1000,
                        cfactor: Optional[torch.Tensor] = None, sun: Optional[torch.Tensor] = None,
                        ncells: Optional[int] = None, out: Optional[RosenbrockResult] = None,
+                       work: Optional[torch.Tensor] = None,
                        stream: Optional[torch.cuda.Stream] = None) -> RosenbrockResult:
         """The reference's Rosenbrock discrete adjoint for every cell
         (kpp_b200_rosenbrock_adj, libraries built on KPP's own generator):
         var and lam [NADJ * NVAR, ld] in place; ICNTRL / RCNTRL in the C
         layout of int/rosenbrock_adj.c; bufsize = trajectory entries per cell
         (the step limit is bufsize - 1); istatus = ISTATUS[1..8], rstatus
-        [3, ld] = Texit, Hexit, Hnew.  The work buffer is allocated here.
+        [3, ld] = Texit, Hexit, Hnew.  work: a float64 device buffer of at
+        least kpp_b200_rosenbrock_adj_work_bytes bytes, else allocated here.
         Asynchronous."""
         f64, i32 = torch.float64, torch.int32
         self._dev(var, f64, "var")
@@ -408,14 +410,18 @@ class Mechanism:
                                    rstatus=torch.empty(3, ld, dtype=f64, device=var.device))
         nbytes = int(self.lib.kpp_b200_rosenbrock_adj_work_bytes(ld, nadj, int(bufsize),
                                                                  int(icntrl[7])))
-        work = torch.empty(max(nbytes // 8, 1), dtype=f64, device=var.device)
+        if work is None:
+            work = torch.empty(max(nbytes // 8, 1), dtype=f64, device=var.device)
+        self._dev(work, f64, "work")
+        if work.numel() * 8 < nbytes:
+            raise KppError(f"work must hold {nbytes} bytes, has {work.numel() * 8}")
         ic = (ctypes.c_int * 20)(*[int(x) for x in icntrl])
         rc = (ctypes.c_double * 20)(*[float(x) for x in rcntrl])
         s = stream if stream is not None else torch.cuda.current_stream(var.device)
         self._check(self.lib.kpp_b200_rosenbrock_adj(
             n, ld, _ptr(var), _ptr(fix), _ptr(temp), _ptr(cfactor), _ptr(sun), _ptr(tstart),
             _ptr(tend), _ptr(atol), _ptr(rtol), nadj, _ptr(lam), ic, rc, int(bufsize),
-            _ptr(work), nbytes, _ptr(out.istatus), _ptr(out.rstatus), _ptr(out.ierr),
+            _ptr(work), work.numel() * 8, _ptr(out.istatus), _ptr(out.rstatus), _ptr(out.ierr),
             _vp(s.cuda_stream)))
         out.work = work  # kept alive until the caller drops the result
         return out

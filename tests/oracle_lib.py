@@ -268,6 +268,48 @@ class RkOracle(IntegratorOracle):
         self.lib.kpprk_solve_cmplx(_p(jr), _p(ji), _p(xr), _p(xi))
 
 
+def adj_lib_path(mech: str, opt: str = "") -> Path:
+    return REF_DIR / f"{mech}_adj" / f"libkppadj_{mech}{opt}.so"
+
+
+class AdjOracle:
+    """The reference's own C RosenbrockADJ (int/rosenbrock_adj.c) on the
+    mechanism's generated model with its Hessian, per cell through
+    oracle/refkpp/batch_driver_adj.c."""
+
+    def __init__(self, mech: str, opt: str = ""):
+        self.lib = ctypes.CDLL(str(adj_lib_path(mech, opt)))
+        self._integrate = self.lib.kppadj_integrate
+        self._integrate.argtypes = ([ctypes.c_int, ctypes.c_int] + [_vp] * 9 + [ctypes.c_int]
+                                    + [_vp] * 3 + [ctypes.c_int] + [_vp] * 3)
+        d = (ctypes.c_int * 5)()
+        self.lib.kppadj_dims(d)
+        self.nvar = d[0]
+
+    def integrate(self, var, fix, temp, tstart, tend, atol, rtol, lam, icntrl, rcntrl, bufsize,
+                  cfactor=None, sun=None):
+        """Returns (var_out, lam_out, istatus [8][n], rstatus [3][n], ierr):
+        ISTATUS[1..8], RSTATUS[1..3]; lam [NADJ * NVAR][n]."""
+        var = np.ascontiguousarray(var, dtype=np.float64).copy()
+        lam = np.ascontiguousarray(lam, dtype=np.float64).copy()
+        n = var.shape[1]
+        nadj = lam.shape[0] // self.nvar
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        fix = f64(fix) if fix is not None and np.size(fix) else np.zeros((1, n))
+        temp, tstart, tend, atol, rtol = f64(temp), f64(tstart), f64(tend), f64(atol), f64(rtol)
+        cfactor, sun = f64(cfactor), f64(sun)
+        ic = np.ascontiguousarray(icntrl, dtype=np.int32)
+        rc = np.ascontiguousarray(rcntrl, dtype=np.float64)
+        ist = np.zeros((8, n), np.int32)
+        rst = np.zeros((3, n))
+        ierr = np.zeros(n, np.int32)
+        with quiet_stdout():
+            self._integrate(n, n, _p(var), _p(fix), _p(temp), _p(cfactor), _p(sun), _p(tstart),
+                            _p(tend), _p(atol), _p(rtol), nadj, _p(lam), _p(ic), _p(rc),
+                            int(bufsize), _p(ist), _p(rst), _p(ierr))
+        return var, lam, ist, rst, ierr
+
+
 def integrator_alternates(kind: str, mech: str, var, fix, temp, tstart, tend, atol, rtol,
                           icntrl, rcntrl, cfactor=None, sun=None):
     """VAR after the same SDIRK or Runge-Kutta integration by the reference

@@ -45,6 +45,19 @@ def test_library_exports_every_declared_entry(mech):
     ctypes.CDLL(str(lib))  # loads without a GPU
 
 
+@pytest.mark.parametrize("mech", ["small_strato", "saprc99"])
+def test_route_library_exports_every_declared_entry(mech):
+    """The libraries built on KPP's own generator (#LANGUAGE CUDA) carry the
+    same C ABI, the Rosenbrock adjoint included."""
+    from kpp_b200 import build
+    lib = build.library_path(mech, "kpp")
+    if not lib.exists():
+        pytest.skip(f"{lib.name} not built (KPP's sources were not found at build time)")
+    missing = [n for n in declared_functions() if n not in exported(lib)]
+    assert not missing, missing
+    ctypes.CDLL(str(lib))
+
+
 @pytest.mark.parametrize("mech", MECHS)
 def test_mechanism_description_matches_reference(mech, golden_dir):
     _skip_on_request(mech)
