@@ -26,6 +26,13 @@
 extern "C" {
 #endif
 
+/* The entry points below are the library's only exported symbols: it is
+   built with hidden visibility, so that the per-device set-up state of each
+   mechanism library stays its own when several are loaded in one process. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 #define KPP_B200_OK 0
 #define KPP_B200_EINVAL 1 /* invalid argument: size, null pointer, ld < ncells */
 #define KPP_B200_ECUDA 2  /* CUDA runtime or launch error (see last_error) */
@@ -374,6 +381,10 @@ int kpp_b200_shuffle_kpp2user(int ncells, int ld, const double *var, int ld_user
 
 /* Text of the last error of this thread's last failing call. */
 const char *kpp_b200_last_error(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

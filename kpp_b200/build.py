@@ -45,8 +45,12 @@ INCLUDE = PKG.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: no FMA contraction, so the double arithmetic rounds like the
 # reference C code built without FMA (x86-64 gcc -O).
+# -fvisibility=hidden: only the C ABI (declared with default visibility in
+# include/kpp_b200.h) is exported, so the function-local statics of the
+# launchers (per-device set-up) are not merged across mechanism libraries
+# loaded in one process.
 NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-diag-suppress", "177"]
+              "-Xcompiler", "-fvisibility=hidden", "-diag-suppress", "177"]
 METHOD_PARTS = [1, 2, 3, 4, 5]
 SDIRK_PART = 6  # the SDIRK integrator
 RK_PART = 7     # the Runge-Kutta integrator (complex LU from <mech>_cmplx.cuh)

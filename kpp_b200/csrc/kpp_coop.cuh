@@ -14,8 +14,13 @@
 //              order (lane streams of packed entries)
 //   LU         the operations of util/sutil.c's loop list-scheduled into
 //              iterations separated by warp barriers
-//   solves     forward and backward substitution, each row's left-to-right sum
-//              owned by one lane and advanced as its operands become final
+//   forward    substitution: each row's left-to-right sum owned by one lane
+//              and advanced as its operands become final
+// The backward substitution is a single dependent chain (each row's first
+// term needs the row just below it), so one lane runs it as the straight-line
+// code of the mechanism header (kpp_solve_bw) while the warp waits: spreading
+// it over the lanes added table reads and barriers to every link of the chain
+// and took half of the kernel's time; on one lane it takes a third less.
 // Only operations that do not depend on each other run side by side, and each
 // value is produced by the operation sequence of the unrolled functions, so the
 // kernel is bit-identical to the thread-per-cell kernel (and performs the
@@ -30,8 +35,6 @@
 // weights from them.  Other mechanisms and inputs use the thread-per-cell
 // kernel.
 #pragma once
-
-#include "kpp_div.cuh"
 
 namespace coop {
 
@@ -51,11 +54,10 @@ struct Cell {
   static constexpr int V1 = A + K::NA;          // ynew, FIX, 1.0
   static constexpr int FCN = V1 + K::NEXT;      // stage Fun; then Yerr and the error terms
   static constexpr int KS = FCN + NVAR;         // stage vectors
-  static constexpr int RY = KS + S * NVAR;      // reciprocals of the U diagonal
-  static constexpr int END = RY + NVAR;
-  // Jac_SP's partial derivatives reuse [FCN, RY) (dead while the matrix is
+  static constexpr int END = KS + S * NVAR;
+  // Jac_SP's partial derivatives reuse [FCN, END) (dead while the matrix is
   // built) when they fit there
-  static constexpr int B = (RY - FCN >= K::NB) ? FCN : END;
+  static constexpr int B = (END - FCN >= K::NB) ? FCN : END;
   static constexpr int TOTAL = (B == FCN) ? END : END + K::NB;
   static_assert(LU_NZ + K::NA >= NREACT, "rate constants are staged in [JVS, V1)");
 };
@@ -203,10 +205,8 @@ __device__ __forceinline__ int warp_min(int v) {
 
 // In-place no-pivot sparse LU; returns k+1 for the first row whose diagonal
 // is zero on entry to its elimination (its original value: util/sutil.c only
-// changes a row during that row's own elimination), 0 on success.  On success
-// ry[i] = 1/U(i,i), the divisors of the backward substitution.
-__device__ __forceinline__ int decomp(const unsigned* __restrict__ tab, double* J, double* ry,
-                                      int lane) {
+// changes a row during that row's own elimination), 0 on success.
+__device__ __forceinline__ int decomp(const unsigned* __restrict__ tab, double* J, int lane) {
   int bad = NVAR;
   for (int i = lane; i < NVAR; i += 32)
     if (J[tab[K::O_DIAG + i]] == 0.0 && i < bad) bad = i;
@@ -235,51 +235,35 @@ __device__ __forceinline__ int decomp(const unsigned* __restrict__ tab, double* 
     n = n_next;
     __syncwarp();
   }
-  for (int i = lane; i < NVAR; i += 32) ry[i] = 1.0 / J[tab[K::O_DIAG + i]];
-  __syncwarp();
   return 0;
 }
 
-// Forward (BACKWARD = false) or backward substitution in place; the backward
-// rows divide by U(i,i) through its reciprocal ry[i] (kpp_div_recip: the
-// same quotient as the division).
-template <bool BACKWARD>
-__device__ __forceinline__ void substitute(const unsigned* __restrict__ tab, const double* J,
-                                           const double* ry, double* X, int lane) {
+// Forward substitution in place (unit lower triangle, KppSolve's first loop).
+__device__ __forceinline__ void forward(const unsigned* __restrict__ tab, const double* J,
+                                        double* X, int lane) {
   constexpr int B = K::LU_BITS, C = K::X_BITS, F = B + 2 * C, CAP = K::SOLVE_CAP;
-  constexpr int OC = BACKWARD ? K::O_CBW : K::O_CFW;
-  constexpr int OS = BACKWARD ? K::O_BW : K::O_FW;
-  constexpr int IT = BACKWARD ? K::IT_BW : K::IT_FW;
   double acc = 0.0;
   int pos = 0;
-  int n = lane_count(tab, OC, 0, lane);
-  for (int it = 0; it < IT; it++) {
+  int n = lane_count(tab, K::O_CFW, 0, lane);
+  for (int it = 0; it < K::IT_FW; it++) {
     unsigned e[CAP];
-    double jv[CAP], xv[CAP], xs[CAP], dv[CAP], yv[CAP];
+    double jv[CAP], xv[CAP], xs[CAP];
 #pragma unroll
-    for (int j = 0; j < CAP; j++) e[j] = (j < n) ? tab[OS + (pos + j) * 32 + lane] : 0u;
+    for (int j = 0; j < CAP; j++) e[j] = (j < n) ? tab[K::O_FW + (pos + j) * 32 + lane] : 0u;
 #pragma unroll
     for (int j = 0; j < CAP; j++) {
-      const unsigned r = (e[j] >> (B + C)) & ((1u << C) - 1);
       jv[j] = J[e[j] & ((1u << B) - 1)];
       xv[j] = X[(e[j] >> B) & ((1u << C) - 1)];
-      xs[j] = X[r];
-      if (BACKWARD) {
-        dv[j] = J[tab[K::O_DIAG + r]];
-        yv[j] = ry[r];
-      }
+      xs[j] = X[(e[j] >> (B + C)) & ((1u << C) - 1)];
     }
-    const int n_next = (it + 1 < IT) ? lane_count(tab, OC, it + 1, lane) : 0;
-    // the running sums; a backward quotient comes from the reciprocal when
-    // its operands are in kpp_div_recip_ok's range, else from the division
+    const int n_next = (it + 1 < K::IT_FW) ? lane_count(tab, K::O_CFW, it + 1, lane) : 0;
+    // the running sums
 #pragma unroll
     for (int j = 0; j < CAP; j++) {
       if (j < n) {
         if ((e[j] >> F) & 1u) acc = xs[j];
-        if (!((e[j] >> (F + 2)) & 1u)) acc = acc - jv[j] * xv[j];
-        if ((e[j] >> (F + 1)) & 1u)
-          X[(e[j] >> (B + C)) & ((1u << C) - 1)] =
-              BACKWARD ? kpp_div_recip(acc, dv[j], yv[j]) : acc;
+        acc = acc - jv[j] * xv[j];
+        if ((e[j] >> (F + 1)) & 1u) X[(e[j] >> (B + C)) & ((1u << C) - 1)] = acc;
       }
     }
     pos += n;
@@ -288,11 +272,13 @@ __device__ __forceinline__ void substitute(const unsigned* __restrict__ tab, con
   }
 }
 
-// Solve (LU) x = b in place, b given in X.
-__device__ __forceinline__ void solve(const unsigned* __restrict__ tab, const double* J,
-                                      const double* ry, double* X, int lane) {
-  substitute<false>(tab, J, ry, X, lane);
-  substitute<true>(tab, J, ry, X, lane);
+// Solve (LU) x = b in place, b given in X: the forward substitution over the
+// warp, the backward one on lane 0.
+__device__ __forceinline__ void solve(const unsigned* __restrict__ tab, const double* J, double* X,
+                                      int lane) {
+  forward(tab, J, X, lane);
+  if (lane == 0) kpp_solve_bw(J, X);
+  __syncwarp();
 }
 
 // ---- vector operations of the integrator (util/blas.c), lane-strided -------
@@ -370,7 +356,7 @@ __device__ int integrate(const unsigned* tab, const double* kc, const Weights& w
         for (;;) {
           const double ghinv = 1.0 / (direction * h * tab_m.Gamma[0]);
           jac_matrix<S>(tab, kc, w.j, sm, ghinv, lane);
-          const int ising = decomp(tab, jvs, sm + L::RY, lane);
+          const int ising = decomp(tab, jvs, lane);
           st.ndec++;
           if (ising == 0) break;
           st.nsng++;
@@ -405,7 +391,7 @@ __device__ int integrate(const unsigned* tab, const double* kc, const Weights& w
           const double hg = direction * h * tab_m.Gamma[s];
           vaxpy(hg, dfdt, kst(s), lane);
         }
-        solve(tab, jvs, sm + L::RY, kst(s), lane);
+        solve(tab, jvs, kst(s), lane);
         st.nsol++;
       }
 

@@ -484,25 +484,25 @@ CoopStream coop_schedule_lu(const Mechanism& m, int B) {
   return st;
 }
 
-// Forward (L, unit diagonal) or backward (U) substitution.  Entry =
-// a | c<<B | r<<(B+C) | start<<(B+2C) | end<<(B+2C+1) | noterm<<(B+2C+2):
-// start: acc = X[r]; a term: acc = acc - J[a]*X[c]; end: X[r] = acc, divided
-// by J[diag r] in the backward phase; noterm: a backward row without terms.
-CoopStream coop_schedule_solve(const Mechanism& m, bool backward, int B, int C) {
+// Forward substitution (L, unit diagonal).  Entry =
+// a | c<<B | r<<(B+C) | start<<(B+2C) | end<<(B+2C+1):
+// start: acc = X[r]; a term: acc = acc - J[a]*X[c]; end: X[r] = acc.  Each
+// row's terms stay on one lane in the row's own order; a row starts once its
+// first operand is final, and a term waits for its operand.  (The backward
+// substitution is one dependent chain -- every row begins with the row just
+// below it -- so the kernel runs it as straight-line code on one lane.)
+CoopStream coop_schedule_forward(const Mechanism& m, int B, int C) {
   const int n = m.nvar;
   std::vector<std::vector<std::pair<int, int>>> terms(n);
-  for (int r = 0; r < n; r++) {
-    const int b = backward ? m.lu_diag[r] + 1 : m.lu_crow[r];
-    const int e = backward ? m.lu_crow[r + 1] : m.lu_diag[r];
-    for (int j = b; j < e; j++) terms[r].push_back({j, m.lu_icol[j]});
-  }
+  for (int r = 0; r < n; r++)
+    for (int j = m.lu_crow[r]; j < m.lu_diag[r]; j++) terms[r].push_back({j, m.lu_icol[j]});
   const int INF = 1 << 30;
   std::vector<int> fin(n, INF);
   std::vector<char> started(n, 0);
   int todo = 0;
   for (int r = 0; r < n; r++) {
-    if (!backward && terms[r].empty()) {
-      fin[r] = -1;  // forward: unchanged, final from the start
+    if (terms[r].empty()) {
+      fin[r] = -1;  // unchanged, final from the start
       started[r] = 1;
     } else {
       todo++;
@@ -513,15 +513,14 @@ CoopStream coop_schedule_solve(const Mechanism& m, bool backward, int B, int C) 
   for (int r = 0; r < n; r++)
     for (auto& t : terms[r]) users[t.second].push_back(r);
   std::vector<int> tail(n, 0);
-  for (int step = 0; step < n; step++) {
-    const int r = backward ? step : n - 1 - step;  // users come after r in the phase
+  for (int r = n - 1; r >= 0; r--) {  // users come after r
     int best = 0;
     for (int w : users[r]) best = std::max(best, tail[w]);
     tail[r] = (int)terms[r].size() + 1 + best;
   }
   std::vector<int> row(kCoopLanes, -1), next_term(kCoopLanes, 0);
   CoopStream st;
-  const unsigned S0 = 1u << (B + 2 * C), E0 = 1u << (B + 2 * C + 1), N0 = 1u << (B + 2 * C + 2);
+  const unsigned S0 = 1u << (B + 2 * C), E0 = 1u << (B + 2 * C + 1);
   for (int it = 0; todo > 0; it++) {
     if (it > 100000) break;  // no progress: cannot happen for a triangular system
     std::vector<int> cnt(kCoopLanes, 0);
@@ -537,7 +536,7 @@ CoopStream coop_schedule_solve(const Mechanism& m, bool backward, int B, int C) 
           int best = -1;
           for (int r = 0; r < n; r++) {
             if (started[r]) continue;
-            const bool ok = terms[r].empty() || fin[terms[r][0].second] < it;
+            const bool ok = fin[terms[r][0].second] < it;
             if (ok && (best < 0 || tail[r] > tail[best])) best = r;
           }
           if (best < 0) break;
@@ -546,14 +545,6 @@ CoopStream coop_schedule_solve(const Mechanism& m, bool backward, int B, int C) 
           next_term[l] = 0;
         }
         const int r = row[l];
-        if (terms[r].empty()) {  // backward row without terms: X[r] = X[r] / J[diag]
-          st.lane[l].push_back((unsigned)r << (B + C) | S0 | E0 | N0);
-          cnt[l]++;
-          fin[r] = it;
-          todo--;
-          row[l] = -1;
-          continue;
-        }
         const int k = next_term[l];
         const auto& t = terms[r][k];
         if (fin[t.second] >= it) break;  // operand not final yet
@@ -729,15 +720,13 @@ void emit_coop_tables(std::ostream& o, const Mechanism& m) {
   std::vector<unsigned> sv = coop_schedule_sums(vsum, vdiag, SL, lv);
   std::vector<unsigned> sj = coop_schedule_sums(jsum, jdiag, SL, lj);
   CoopStream lu = coop_schedule_lu(m, B);
-  CoopStream fw = coop_schedule_solve(m, false, B, C);
-  CoopStream bw = coop_schedule_solve(m, true, B, C);
+  CoopStream fw = coop_schedule_forward(m, B, C);
   std::vector<unsigned> diag(m.lu_diag.begin(), m.lu_diag.begin() + nvar);
   struct Part { const char* name; std::vector<unsigned> words; };
   std::vector<Part> parts = {
       {"PF", fa}, {"WF", wa}, {"PJ", fb}, {"WJ", wb}, {"SV", sv}, {"SJ", sj},
       {"CLU", lu.counts()}, {"LU", lu.interleaved(0)}, {"CFW", fw.counts()},
-      {"FW", fw.interleaved(0)}, {"CBW", bw.counts()}, {"BW", bw.interleaved(0)},
-      {"DIAG", diag}};
+      {"FW", fw.interleaved(0)}, {"DIAG", diag}};
   long total_words = 0;
   for (auto& p : parts) total_words += (long)p.words.size();
   // one cell of the six-stage method beside the tables must fit the 227 KB of
@@ -773,7 +762,7 @@ void emit_coop_tables(std::ostream& o, const Mechanism& m) {
     << "constexpr int LV = " << lv << ", LJ = " << lj << ";  // entries per lane of the sums ("
     << sum_terms_v << " and " << sum_terms_j << " terms)\n"
     << "constexpr int IT_LU = " << lu.count.size() << ", IT_FW = " << fw.count.size()
-    << ", IT_BW = " << bw.count.size() << ";  // iterations\n"
+    << ";  // iterations\n"
     << "constexpr int LU_BITS = " << B << ", X_BITS = " << C << ";\n"
     << "constexpr int LU_CAP = " << kCoopLuCap << ", SOLVE_CAP = " << kCoopSolveCap
     << ";  // entries per lane per iteration\n";
@@ -1152,10 +1141,12 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
     }
     o << "  (void)a;\n  return 0;\n}\n\n";
 
-    // ---- KppSolve, unrolled
-    o << "// Solve (LU) x = b in place, b given in X.\n"
+    // ---- KppSolve, unrolled: the forward and the backward substitution as
+    // functions of their own (the warp-per-cell kernel runs the backward one
+    // on a single lane), and kpp_solve = both
+    o << "// Forward substitution of KppSolve in place (L x = b, unit diagonal).\n"
          "template <class TJ, class TX>\n"
-         "__device__ KPP_MECH_INLINE void kpp_solve(const TJ& JVS, TX& X) {\n";
+         "__device__ KPP_MECH_INLINE void kpp_solve_fw(const TJ& JVS, TX& X) {\n";
     for (int i = 0; i < nvar; i++) {
       int b = m.lu_crow[i], e = m.lu_diag[i];
       if (b < e) {
@@ -1167,6 +1158,10 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
         o << "  X[" << i << "] = " << print(sum) << ";\n";
       }
     }
+    o << "}\n\n"
+         "// Backward substitution of KppSolve in place (U x = b).\n"
+         "template <class TJ, class TX>\n"
+         "__device__ KPP_MECH_INLINE void kpp_solve_bw(const TJ& JVS, TX& X) {\n";
     for (int i = nvar - 1; i >= 0; i--) {
       P sum = leaf("X[" + std::to_string(i) + "]");
       for (int j = m.lu_diag[i] + 1; j < m.lu_crow[i + 1]; j++)
@@ -1176,7 +1171,13 @@ bool emit_cuda(const Mechanism& m, const std::string& out_prefix) {
       ops_solve += count_ops(sum);
       o << "  X[" << i << "] = " << print(sum) << ";\n";
     }
-    o << "}\n#endif  // KPP_EXTERNAL_ARITHMETIC\n\n";
+    o << "}\n\n"
+         "// Solve (LU) x = b in place, b given in X.\n"
+         "template <class TJ, class TX>\n"
+         "__device__ __forceinline__ void kpp_solve(const TJ& JVS, TX& X) {\n"
+         "  kpp_solve_fw(JVS, X);\n"
+         "  kpp_solve_bw(JVS, X);\n"
+         "}\n#endif  // KPP_EXTERNAL_ARITHMETIC\n\n";
   }
 
   // ---- KppDecompCmplxR / KppSolveCmplxR (util/sutil.c:28-90), unrolled.

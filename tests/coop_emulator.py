@@ -4,7 +4,9 @@ kppcu writes, into each mechanism's header, the tables that the warp-per-cell
 kernel (kpp_b200/csrc/kpp_coop.cuh) stages in shared memory: the product
 factors and weights of Fun and Jac_SP, the lane streams of the Vdot and
 Jacobian sums, and the iteration counts and lane streams of the LU
-factorisation and of the forward and backward substitutions.  This module
+factorisation and of the forward substitution (the backward substitution
+runs on one lane as the header's straight-line kpp_solve_bw, restated here
+row by row in KppSolve's order).  This module
 reads those tables back from the header and executes them the way the kernel
 does -- iteration by iteration, lane by lane, in IEEE double arithmetic -- so
 that tests can require the results to equal the reference's own generated
@@ -137,24 +139,28 @@ class CoopTables:
         self._iterate(self.O_CLU, self.O_LU, self.IT_LU, step)
         return 0
 
-    def solve(self, jvs, x):
-        """(LU) x = b in place, b given in x."""
+    def solve(self, jvs, x, lu_pattern):
+        """(LU) x = b in place, b given in x: the forward substitution from the
+        tables, then the backward one in KppSolve's order (src/gen.c:1960-2034:
+        each row's terms left to right, then the division by the diagonal) over
+        lu_pattern = (LU_IROW, LU_ICOL, LU_CROW, LU_DIAG)."""
         b, c = self.LU_BITS, self.X_BITS
-        diag = self.tab[self.O_DIAG:self.O_DIAG + self.nvar]
         acc = [0.0] * LANES
 
-        def make(backward):
-            def step(lane, e):
-                a, cc = e & ((1 << b) - 1), (e >> b) & ((1 << c) - 1)
-                r = (e >> (b + c)) & ((1 << c) - 1)
-                f = b + 2 * c
-                if (e >> f) & 1:
-                    acc[lane] = x[r]
-                if not (e >> (f + 2)) & 1:
-                    acc[lane] = acc[lane] - jvs[a] * x[cc]
-                if (e >> (f + 1)) & 1:
-                    x[r] = acc[lane] / jvs[diag[r]] if backward else acc[lane]
-            return step
+        def step(lane, e):
+            a, cc = e & ((1 << b) - 1), (e >> b) & ((1 << c) - 1)
+            r = (e >> (b + c)) & ((1 << c) - 1)
+            f = b + 2 * c
+            if (e >> f) & 1:
+                acc[lane] = x[r]
+            acc[lane] = acc[lane] - jvs[a] * x[cc]
+            if (e >> (f + 1)) & 1:
+                x[r] = acc[lane]
 
-        self._iterate(self.O_CFW, self.O_FW, self.IT_FW, make(False))
-        self._iterate(self.O_CBW, self.O_BW, self.IT_BW, make(True))
+        self._iterate(self.O_CFW, self.O_FW, self.IT_FW, step)
+        _, icol, crow, diag = lu_pattern
+        for i in range(self.nvar - 1, -1, -1):
+            v = x[i]
+            for j in range(diag[i] + 1, crow[i + 1]):
+                v = v - jvs[j] * x[icol[j]]
+            x[i] = v / jvs[diag[i]]

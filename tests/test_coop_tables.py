@@ -50,7 +50,9 @@ def test_lu_and_solves_reproduce_kppdecomp_and_kppsolve(mech, golden_dir):
     t = _tables(mech)
     if not lib_path(mech).exists():
         pytest.skip("oracle libraries not present")
-    ref = OracleLib(mech).lib
+    oracle = OracleLib(mech)
+    ref = oracle.lib
+    pattern = oracle.lu_pattern()
     ref.KppDecomp.argtypes = [ctypes.c_void_p]
     ref.KppSolve.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     g = np.load(golden_dir / f"funjac_{mech}.npz")
@@ -72,7 +74,7 @@ def test_lu_and_solves_reproduce_kppdecomp_and_kppsolve(mech, golden_dir):
             xw = np.ascontiguousarray(x.copy())
             ref.KppSolve(_p(want), _p(xw))
             xg = list(x)
-            t.solve(got, xg)
+            t.solve(got, xg, pattern)
             np.testing.assert_array_equal(np.array(xg), xw)
             checked += 1
     assert checked > 0
