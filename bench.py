@@ -55,13 +55,26 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "saprc99 cell-steps/s at 2^20 cells, learned-scheduled vs plain, same accuracy"
 UNIT = "cell-steps/s"
-# DRAM traffic of the thread-per-cell Rosenbrock kernel per internal step at
-# full residency (ncu dram__bytes_read.sum + dram__bytes_write.sum of one
-# launch over 2^17 fresh saprc99 cells, every thread slot of the GPU busy:
-# 990.0 + 311.4 GB over 6,480,123 internal steps,
-# profiles/rosenbrock_kernel_thread_saprc99_2p17_traffic.md): the per-cell
-# work set (LU factors, stage vectors) streams through L2 to HBM.
-DRAM_BYTES_PER_INTERNAL_STEP = (989962676736 + 311353660160) / 6480123
+# DRAM traffic per internal step of each Rosenbrock kernel at full residency
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch over fresh
+# saprc99 cells):
+#   thread per cell: 2^17 cells, every thread slot of the GPU busy: 990.0 +
+#     311.4 GB over 6,480,123 internal steps
+#     (profiles/rosenbrock_kernel_thread_saprc99_2p17_traffic.md): the
+#     per-cell work set (LU factors, stage vectors) streams through L2 to HBM;
+#   warp per cell: 2048 cells (every SM's 12 cells busy, then a tail):
+#     2.04 MB read, 0 written over 101,110 internal steps
+#     (profiles/kernel_coop_saprc99_2048_fresh.md): the work set stays in
+#     shared memory; what remains is the cells' inputs and outputs.
+DRAM_BYTES_PER_INTERNAL_STEP = {"thread": (989962676736 + 311353660160) / 6480123,
+                                "warp": 2039040 / 101110}
+TRAFFIC_SOURCE = {
+    "thread": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one rosenbrock_kernel "
+              "launch over 2^17 fresh cells at full residency (profiles/), per internal step, "
+              "times this launch's internal steps",
+    "warp": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one warp-per-cell kernel "
+            "launch over 2048 fresh cells, every SM's cells busy (profiles/), per internal "
+            "step, times this launch's internal steps"}
 # Compulsory bytes per cell-step: VAR in and out, FIX, TEMP, CFACTOR, SUN,
 # TSTART, TEND, Hstart in; ISTATUS, RSTATUS, IERR out (saprc99: 74 + 74 + 5 +
 # 6 doubles, 9 ints, 2 doubles).
@@ -365,9 +378,15 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
     if args.queue != "tuned":
         mech.set_queue_lanes(args.queue == "lanes")  # an explicit choice wins
     queue = "lanes" if mech.queue_lanes() else "warps"
-    kernel = mech.kernel()
     wl = workloads.for_mechanism(mech, args.workload, args.ncells, seed=shard_seed(rank))
     n = wl.ncells
+    # the kernel choice of the headline arms: the tuning record's, else the
+    # command line's (auto: the library's automatic choice)
+    arm_kernel = shape["kernel"] if shape else args.kernel
+    mech.set_kernel("warp")
+    has_warp = mech.kernel() == "warp" and wl.sun is not None
+    mech.set_kernel(arm_kernel)
+    kernel = ("warp" if has_warp else "thread") if arm_kernel == "auto" else arm_kernel
     D = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     var = D(wl.var)
     fix, temp = D(wl.fix), D(wl.temp)
@@ -406,9 +425,10 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         each cell's best starting step among the training candidates, queued
         by its true step count)."""
 
-        def __init__(self, learned, fixed=None):
+        def __init__(self, learned, fixed=None, kernel=None):
             self.learned = learned
             self.fixed = fixed
+            self.kernel = kernel  # a kernel choice for this arm's launches, else the tuned one
             self.out = None
             self.hs = torch.zeros(n, dtype=torch.float64, device=dev)
             self.hs_plan = torch.empty(n, dtype=torch.float64, device=dev)
@@ -431,10 +451,14 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                     var, fix, temp, t0, wl.dt, 1, atol, rtol, wl.ipar, wl.rpar, cfactor=cf,
                     sun=sun, hstart=self.fixed[0], order=self.fixed[1], out=self.out)
             elif not self.learned:
+                if self.kernel is not None:
+                    mech.set_kernel(self.kernel)
                 if ev:
                     ev[0].record(stream)
                 self.out = mech.rosenbrock(var, fix, temp, t0, t1, atol, rtol, wl.ipar, wl.rpar,
                                            cfactor=cf, sun=sun, hstart=warm, out=self.out)
+                if self.kernel is not None:
+                    mech.set_kernel(arm_kernel)
             else:
                 sched.plan(var, temp, t0, cfactor=cf, sun=sun, tend=t1, hstart=self.hs_plan,
                            order=self.order)
@@ -493,7 +517,13 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
                     "istatus_sum": dict(zip(["nfun", "njac", "nstp", "nacc", "nrej", "ndec",
                                              "nsol", "nsng"], map(int, self.ist)))}
 
-    plain = Arm(False).run()
+    # the plain form: one launch per step with the library's automatic kernel
+    # choice (the warp-per-cell kernel where the mechanism has it), and, for
+    # comparison, the thread-per-cell kernel's plain launch
+    plain_kernel = ("warp" if has_warp else "thread") if args.kernel == "auto" else args.kernel
+    plain = Arm(False, kernel=args.kernel).run()
+    plain_thread = (Arm(False, kernel="thread").run()
+                    if fresh and plain_kernel != "thread" and args.plain_thread else None)
     # the work queue alone: the plain controls (Hstart = STEPMIN) and cells in
     # batch order, so its gain over plain is the queue's, none of it learned
     queued = (Arm(False, fixed=(torch.zeros(n, dtype=torch.float64, device=dev),
@@ -545,7 +575,7 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
              + nsol * opsd.get("solve", 0) + nstp * vec["per_attempt"] + njac * vec["per_step"])
     # the dominant kernel's launches only (the scheduling pass excluded)
     achieved_tflops = flops / (head.kernel_ms / 1e3) / 1e12
-    traffic_per_launch = DRAM_BYTES_PER_INTERNAL_STEP * nstp / args.steps
+    traffic_per_launch = DRAM_BYTES_PER_INTERNAL_STEP[kernel] * nstp / args.steps
     peak_fma, peak_muladd = fp64_peak(LIB / "libkpp_b200_util.so")
 
     # ---- end to end through the public API with host buffers (pinned host
@@ -652,6 +682,8 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         torch.cuda.synchronize()
         sched_block.update({
             "speedup_vs_plain": learned.value / plain.value,
+            "speedup_vs_plain_thread": (None if plain_thread is None
+                                        else learned.value / plain_thread.value),
             "queue_cell_order": None if queued is None else {
                 "what": "kpp_b200_rosenbrock_chain, Hstart = STEPMIN, cells in batch order "
                         f"({queue} queue): the work queue without the scheduler",
@@ -735,17 +767,19 @@ def run_cuda_arm(args, rank, world, local_rank, pool=None):
         "impl": "kpp_b200",
         "gpu_launches": args.steps * (launches_learned if learned is not None
                                       else (2 if kernel == "warp" else 1)),
-        "plain": plain.summary(),
+        "plain": dict(plain.summary(), kernel={"thread": "thread per cell",
+                                                "warp": "warp per cell"}[plain_kernel]),
+        "plain_thread": None if plain_thread is None else dict(
+            plain_thread.summary(), kernel="thread per cell",
+            bit_identical_to_plain=bool(np.array_equal(plain_thread.var_out, plain.var_out)
+                                        and np.array_equal(plain_thread.ierr, plain.ierr))),
         "learned": learned.summary() if learned is not None else None,
         "scheduler": sched_block,
         "stats": head.summary(),
         "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": peak_fma,
                      "unit": "TFLOP/s", "frac": achieved_tflops / peak_fma if peak_fma > 0 else None,
                      "traffic": traffic_per_launch,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                                       "one rosenbrock_kernel launch over 2^17 fresh cells at "
-                                       "full residency (profiles/), per internal step, times "
-                                       "this launch's internal steps",
+                     "traffic_source": TRAFFIC_SOURCE[kernel],
                      "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL_STEP * n,
                      "kernel_ms_per_launch": head.kernel_ms / args.steps,
                      "peak_source": "measured on this GPU by the DFMA throughput kernel "
@@ -1344,6 +1378,8 @@ def main():
                     help="cells compared with the FP64 RTOL 1e-10 solution (on the GPU)")
     ap.add_argument("--accuracy-cpu-cells", type=int, default=64,
                     help="of those, cells also solved by the CPU oracle as a cross-check")
+    ap.add_argument("--no-plain-thread", dest="plain_thread", action="store_false",
+                    help="skip the thread-per-cell plain arm beside the automatic plain arm")
     ap.add_argument("--no-queue-arm", dest="queue_arm", action="store_false",
                     help="skip the work-queue arm in cell order with the plain controls")
     ap.add_argument("--no-ceiling", dest="ceiling", action="store_false",

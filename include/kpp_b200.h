@@ -325,9 +325,10 @@ int kpp_b200_decomp_solve(int ncells, int ld, double *jvs, double *x,
  * cell, or no SUN-dependent rates; no rates of time or concentrations) of
  * mechanisms with at most 1024 LU entries; other launches use kernel 1.  Both
  * kernels give bit-identical results.  Automatic selects kernel 2 for such
- * launches of at most kpp_b200_get_auto_warp_cells() cells and kernel 1
- * otherwise: the thread-per-cell kernel needs about 150k cells to fill a
- * B200, the warp-per-cell kernel 1776.  No counterpart in the reference.
+ * launches of at most kpp_b200_get_auto_warp_cells() cells (by default every
+ * size for mechanisms with a per-cell work buffer: on B200 with saprc99 it
+ * measured faster from 2^11 to 2^20 cells) and kernel 1 otherwise.  No
+ * counterpart in the reference.
  * kpp_b200_get_kernel returns the configured kernel (1 or 2; 1 for
  * automatic). */
 int kpp_b200_set_kernel(int which);
@@ -345,8 +346,8 @@ int kpp_b200_get_queue_lanes(void);
 
 /* The automatic choice's limit (process-wide): launches of at most `ncells`
  * cells use the warp-per-cell kernel when they can (0: never).  The autotuner
- * (kpp_b200/autotune.py) measures the crossing point per device and
- * mechanism.  No counterpart in the reference. */
+ * (kpp_b200/autotune.py) measures both kernels per device, mechanism and
+ * workload.  No counterpart in the reference. */
 int kpp_b200_set_auto_warp_cells(int ncells);
 int kpp_b200_get_auto_warp_cells(void);
 

@@ -233,7 +233,7 @@ def build_util(force: bool = False) -> Path:
     flags = ARCH + ["-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
                     "-lineinfo"]
     stamp = BUILD / "util.stamp"
-    digest = _hash_files([src, CSRC / "kpp_div.cuh", CSRC / "kpp_ratelaws.cuh"], " ".join(flags))
+    digest = _hash_files([src, CSRC / "kpp_ratelaws.cuh"], " ".join(flags))
     if not force and lib.exists() and stamp.exists() and stamp.read_text() == digest:
         return lib
     _run([nvcc()] + flags + [str(src), "-o", str(lib)])

@@ -16,11 +16,12 @@
 //              iterations separated by warp barriers
 //   forward    substitution: each row's left-to-right sum owned by one lane
 //              and advanced as its operands become final
-// The backward substitution is a single dependent chain (each row's first
-// term needs the row just below it), so one lane runs it as the straight-line
-// code of the mechanism header (kpp_solve_bw) while the warp waits: spreading
-// it over the lanes added table reads and barriers to every link of the chain
-// and took half of the kernel's time; on one lane it takes a third less.
+// The backward substitution is close to one dependent chain (the rows of the
+// dense trailing block each begin with the row just below them), so one lane
+// runs it as the mechanism header's straight-line kpp_solve_bw while the warp
+// waits.  Spread over the lanes, every link of the chain paid table reads and
+// a warp barrier, and the phase took half of the kernel's time; on one lane
+// the kernel runs 1.8x faster (saprc99, 2^17 cells).
 // Only operations that do not depend on each other run side by side, and each
 // value is produced by the operation sequence of the unrolled functions, so the
 // kernel is bit-identical to the thread-per-cell kernel (and performs the
@@ -65,10 +66,16 @@ struct Cell {
 constexpr size_t kTabBytes = ((size_t)K::TAB_WORDS * 4 + 15) / 16 * 16;
 constexpr size_t kTablesBytes = kTabBytes + (size_t)K::NKC * 8;
 
+// Warps (cells) of a CTA: as many cells as shared memory holds beside the
+// tables, at most kMaxWarps.  For mechanisms of saprc99's size the phases'
+// staged operands need about 168 registers per thread, which 12 warps of 32
+// threads allow (at 13 warps ptxas caps the kernel at 128 registers and it
+// spills 2.4 KB per thread); small mechanisms take up to 32 cells.
+constexpr int kMaxWarps = LU_NZ > 256 ? 12 : 32;
 template <int S>
 constexpr int warps_per_cta() {
   const long w = ((long)kSmemMax - (long)kTablesBytes) / ((long)Cell<S>::TOTAL * 8);
-  return w > 32 ? 32 : (w < 1 ? 0 : (int)w);
+  return w > kMaxWarps ? kMaxWarps : (w < 1 ? 0 : (int)w);
 }
 
 template <int S>

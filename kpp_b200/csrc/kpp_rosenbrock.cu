@@ -57,7 +57,9 @@
 // Default of the automatic kernel choice's cell limit (kpp_b200_set_auto_warp_cells).
 #ifndef KPP_COOP_MAX_CELLS
 #if defined(KPP_SCRATCH)
-#define KPP_COOP_MAX_CELLS 32768  // the crossing point measured for saprc99 on B200
+// saprc99 on B200: the warp-per-cell kernel measured faster than the
+// thread-per-cell one at every batch size from 2^11 to 2^20 cells
+#define KPP_COOP_MAX_CELLS 0x7fffffff
 #else
 #define KPP_COOP_MAX_CELLS 0
 #endif

@@ -1,8 +1,7 @@
 // Measurement helpers for the benchmark: the FP64 peak of this GPU, measured
-// with a throughput kernel (no vendor figure for FP64 is assumed); the device
-// self-test of kpp_div.cuh's division through a reciprocal; and a batched
-// evaluation of the controllers' pow (kpp_ratelaws.cuh's kpp_pow_cr) beside
-// the CUDA math library's, for their tests.
+// with a throughput kernel (no vendor figure for FP64 is assumed); and a
+// batched evaluation of the controllers' pow (kpp_ratelaws.cuh's kpp_pow_cr)
+// beside the CUDA math library's, for their tests.
 //
 //   kind 0: fused multiply-add (DFMA), 2 flops per instruction
 //   kind 1: separate multiply and add (DMUL + DADD), 1 flop per instruction;
@@ -10,10 +9,8 @@
 //           built without FMA contraction
 #include <cuda_runtime.h>
 
-#include <cstdint>
 #include <cstdio>
 
-#include "kpp_div.cuh"
 #include "kpp_ratelaws.cuh"
 
 namespace {
@@ -48,45 +45,6 @@ __global__ void __launch_bounds__(256) fp64_muladd_kernel(double* out, int iters
   if (s == 12345.678) out[0] = s;
 }
 
-// Operands for the division self-test: a counter-based hash per sample
-// (splitmix64's finaliser) for the sign, significand and exponent.
-__device__ __forceinline__ uint64_t mix64(uint64_t x) {
-  x ^= x >> 33;
-  x *= 0xff51afd7ed558ccdULL;
-  x ^= x >> 33;
-  x *= 0xc4ceb9fe1a85ec53ULL;
-  x ^= x >> 33;
-  return x;
-}
-
-__device__ __forceinline__ double operand(uint64_t r, int emin, int emax) {
-  const int e = emin + (int)((r >> 52) % (uint64_t)(emax - emin + 1));
-  return __longlong_as_double(
-      (long long)(((r >> 63) << 63) | ((uint64_t)(e + 1023) << 52) | (r & 0xFFFFFFFFFFFFFULL)));
-}
-
-// mode 0: random operands; 1: divisors with a significand of all ones, or
-// nearly; 2: divisors next to a power of two; 3: dividends a = RN(q b), so
-// that quotients sit next to representable numbers.
-__global__ void __launch_bounds__(256) division_check_kernel(uint64_t seed, long long n, int emin,
-                                                             int emax, int mode,
-                                                             unsigned long long* bad) {
-  unsigned long long local = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const uint64_t r1 = mix64(seed * 0x9E3779B97F4A7C15ULL + 2 * (uint64_t)i);
-    const uint64_t r2 = mix64(seed * 0x9E3779B97F4A7C15ULL + 2 * (uint64_t)i + 1);
-    double a = operand(r1, emin, emax), b = operand(r2, emin, emax);
-    const long long bb = __double_as_longlong(b) & ~0xFFFFFFFFFFFFFLL;
-    if (mode == 1) b = __longlong_as_double(bb | (0xFFFFFFFFFFFFFLL - (long long)(r2 & 0xFF)));
-    if (mode == 2) b = __longlong_as_double(bb | (long long)(r2 & 0xFF));
-    if (mode == 3) a = __dmul_rn(operand(r1 | 1, -20, 20), b);
-    const double y = 1.0 / b;
-    if (__double_as_longlong(kpp_div_recip(a, b, y)) != __double_as_longlong(a / b)) local++;
-  }
-  if (local) atomicAdd(bad, local);
-}
-
 __global__ void __launch_bounds__(256) pow_kernel(long long n, const double* x, const double* y,
                                                   double* out, int which) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -113,26 +71,6 @@ int kpp_b200_pow_batch(long long n, const double* x, const double* y, double* ou
       n, x, y, out, which);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
-
-// Self-test of the division through a reciprocal (kpp_div.cuh): the number of
-// n samples (operand exponents in [emin, emax], the given mode) for which it
-// differs from the division a / b in any bit; < 0 on error.
-long long kpp_b200_check_division(unsigned long long seed, long long n, int emin, int emax,
-                                  int mode) {
-  if (n < 0 || emin < -1022 || emax > 1023 || emin > emax || mode < 0 || mode > 3) return -1;
-  unsigned long long* bad = nullptr;
-  if (cudaMalloc(&bad, sizeof *bad) != cudaSuccess) return -1;
-  cudaMemset(bad, 0, sizeof *bad);
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  division_check_kernel<<<sms * 8, 256>>>(seed, n, emin, emax, mode, bad);
-  unsigned long long h = 0;
-  const cudaError_t e = cudaMemcpy(&h, bad, sizeof h, cudaMemcpyDeviceToHost);
-  cudaFree(bad);
-  return e == cudaSuccess ? (long long)h : -1;
-}
-
 
 // Measured FP64 throughput in TFLOP/s (best of `reps` launches); < 0 on error.
 double kpp_b200_fp64_peak_tflops(int kind, int reps) {

@@ -351,9 +351,10 @@ void emit_dtable(std::ostream& o, const char* name, const std::vector<double>& v
 //             pivot; pivot row times the multiplier subtracted) as a dependency
 //             graph, list-scheduled by longest remaining path into iterations
 //             separated by warp barriers, each iteration of one kind
-//   solves    forward and backward substitution: a lane owns a row's
-//             left-to-right sum and runs its terms as soon as their operands
-//             are final (written by another lane in an earlier iteration)
+//   forward   substitution: a lane owns a row's left-to-right sum and runs
+//             its terms as soon as their operands are final (written by
+//             another lane in an earlier iteration); the backward substitution
+//             runs on one lane as the unrolled kpp_solve_bw
 // All tables are 32-bit words in one array that each CTA stages in shared
 // memory.  A phase that iterates holds, per iteration, how many entries each
 // lane runs (4-bit counts, eight lanes per word) and, per lane, its entries in
