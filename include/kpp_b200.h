@@ -327,8 +327,9 @@ int kpp_b200_decomp_solve(int ncells, int ld, double *jvs, double *x,
  * kernels give bit-identical results.  Automatic selects kernel 2 for such
  * launches of at most kpp_b200_get_auto_warp_cells() cells (by default every
  * size for mechanisms with a per-cell work buffer: on B200 with saprc99 it
- * measured faster from 2^11 to 2^20 cells) and kernel 1 otherwise.  No
- * counterpart in the reference.
+ * measured faster from 2^11 to 2^20 cells), except single calls given a
+ * per-cell Hstart (warm-started short calls, where the thread kernel measured
+ * 4.7x faster), and kernel 1 otherwise.  No counterpart in the reference.
  * kpp_b200_get_kernel returns the configured kernel (1 or 2; 1 for
  * automatic). */
 int kpp_b200_set_kernel(int which);

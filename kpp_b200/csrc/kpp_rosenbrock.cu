@@ -828,6 +828,13 @@ bool use_coop(const LaunchArgs& a) {
   if (!coop_supports(a)) return false;
   if (g_kernel_choice == 2) return true;
   if (g_kernel_choice == 1) return false;
+  // A single call warm-started with per-cell Hstart (a host model's time
+  // loop passing the previous call's Hexit) takes a few internal steps, and
+  // the warp kernel re-stages every cell for each such call: measured on
+  // B200 with saprc99 at 2^17 cells, a warm 600 s call took 203 ms there and
+  // 43 ms on the thread kernel (3.3 internal steps per cell).  Those go to
+  // the thread kernel; cold calls and the chained entry keep the warp kernel.
+  if (a.hstart && !a.queue) return false;
   return a.ncells <= g_coop_max_cells.load();
 #else
   (void)a;
