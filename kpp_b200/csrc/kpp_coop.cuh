@@ -21,7 +21,7 @@
 // runs it as the mechanism header's straight-line kpp_solve_bw while the warp
 // waits.  Spread over the lanes, every link of the chain paid table reads and
 // a warp barrier, and the phase took half of the kernel's time; on one lane
-// the kernel runs 1.8x faster (saprc99, 2^17 cells).
+// the kernel runs about twice as fast (saprc99, 2^17 cells).
 // Only operations that do not depend on each other run side by side, and each
 // value is produced by the operation sequence of the unrolled functions, so the
 // kernel is bit-identical to the thread-per-cell kernel (and performs the
