@@ -63,11 +63,11 @@ UNIT = "cell-steps/s"
 #     (profiles/rosenbrock_kernel_thread_saprc99_2p17_traffic.md): the
 #     per-cell work set (LU factors, stage vectors) streams through L2 to HBM;
 #   warp per cell: 2048 cells (every SM's 12 cells busy, then a tail):
-#     2.04 MB read, 0 written over 101,110 internal steps
+#     1.75 MB read, 0 written over 101,110 internal steps
 #     (profiles/kernel_coop_saprc99_2048_fresh.md): the work set stays in
 #     shared memory; what remains is the cells' inputs and outputs.
 DRAM_BYTES_PER_INTERNAL_STEP = {"thread": (989962676736 + 311353660160) / 6480123,
-                                "warp": 2039040 / 101110}
+                                "warp": 1750528 / 101110}
 TRAFFIC_SOURCE = {
     "thread": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one rosenbrock_kernel "
               "launch over 2^17 fresh cells at full residency (profiles/), per internal step, "
